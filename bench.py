@@ -1,0 +1,353 @@
+"""Benchmark: 3-D 7-point Laplacian, 512^3 interior, FP64, on one B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--dtype float64|float32] [--temporal T]
+
+A *step* is one sweep of the stencil over the 512^3 grid (``launch_lap7``
+with ping-pong buffers), inputs resident in HBM.  ``value`` is GPoints/s =
+interior points x steps / device time (CUDA events on the launching stream,
+max over ranks).  Arrays (1.15 GB each) are far larger than the 126 MB L2,
+so no flush is needed between sweeps.
+
+``e2e`` times the configured solve through the public API with host buffers:
+per step, the initial field is copied from pinned host memory, 50 sweeps run
+through ``launch_lap7`` and the result is read back.
+
+``--impl reference`` times the reference's CPU algorithm (the NumPy
+restatement in oracle/, the reference's own NumPy executor cannot travel)
+on all host cores, on a bounded z-slab sample of the same grid.
+
+With N > 1 (torchrun), every rank runs its own independent 512^3 solve
+("replicas only": the path has no data exchange); ``value`` is the sum.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (os.path.join(ROOT, "cutile-stencil-dsl_b200"), ROOT, os.path.join(ROOT, "tests")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+N_INTERIOR = 512
+SOLVE_STEPS = 50
+METRIC = "GPts/s (3-D 7-pt 512^3 sweep)"
+
+
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx = float(parts[2])
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _compile(dtype: str, temporal: int):
+    import stencil_defs as D
+    from cutile import compile as stencil_compile
+    from cutile import stencil
+
+    fn = stencil(ndim=3, order=2, dtype=dtype)(D.lap7)
+    return stencil_compile(fn, temporal_blocking=temporal > 1,
+                           temporal_steps=temporal if temporal > 1 else None)
+
+
+def _init_field(shape, halo, dtype, rank: int):
+    import numpy as np
+
+    u = np.zeros(shape, dtype=dtype)
+    inner = tuple(slice(h, s - h) for h, s in zip(halo, shape))
+    rng = np.random.default_rng(1 + rank)
+    u[inner] = rng.standard_normal(tuple(s - 2 * h for h, s in zip(halo, shape))).astype(dtype)
+    return u
+
+
+def run_ours(args) -> dict:
+    import numpy as np
+    import torch
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", init_method="env://")
+    np_dtype = np.float64 if args.dtype == "float64" else np.float32
+    r = _compile(args.dtype, args.temporal)
+    T = r.temporal_steps
+    halo = r.halo_widths
+    shape = tuple(N_INTERIOR + 2 * h for h in halo)
+    npts = N_INTERIOR ** 3
+    u0 = _init_field(shape, halo, np_dtype, rank)
+    mod = r.load_module()
+    launch = mod.launch_lap7
+    a = torch.from_numpy(u0).cuda()
+    b = torch.zeros_like(a)
+    stream = torch.cuda.current_stream()
+
+    # warm-up (JIT load, occupancy, clocks)
+    for _ in range(args.warmup):
+        launch(a, b)
+        a, b = b, a
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            launch(a, b)
+            a, b = b, a
+        ev1.record(stream)
+        barrier()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    clocks = clk.summary()
+    ms_per_step = ms / args.steps
+    gpts = npts * T * args.steps / (ms / 1e3) / 1e9 * world
+    itemsize = np.dtype(np_dtype).itemsize
+    alg_bytes = 2 * itemsize * npts  # one read + one write per point per launch
+    achieved = alg_bytes / (ms_per_step / 1e3) / 1e9
+    peak, peak_kind = _peaks()
+
+    # end-to-end: pinned host field -> device, 50-sweep solve, result -> host
+    host_in = torch.from_numpy(u0).pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    e2e_steps = 2
+    sweeps = max(1, SOLVE_STEPS // T)
+    for it in range(e2e_steps + 1):
+        if it == 1:
+            barrier()
+            t0 = time.perf_counter()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        a.copy_(host_in, non_blocking=True)
+        for _ in range(sweeps):
+            launch(a, b)
+            a, b = b, a
+        host_out.copy_(a, non_blocking=True)
+        torch.cuda.synchronize()
+    e1 = torch.cuda.Event(enable_timing=True)
+    e1.record(stream)
+    barrier()
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    e2e_wall = (time.perf_counter() - t0) * 1e3 / e2e_steps
+    e2e_ms = max(e2e_ms, e2e_wall)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_gpts = npts * T * sweeps / (e2e_ms / 1e3) / 1e9 * world
+
+    traffic = _profiled_traffic(args.dtype, T)
+    cpu = cpu_baseline(np_dtype) if (rank == 0 and world == 1 and not args.no_cpu) else None
+    line = {
+        "metric": METRIC, "value": round(gpts, 3), "unit": "GPts/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 5),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.dtype == "float64" else "f32", "data": "synthetic",
+        "config": {"workload": f"3-D 7-point Laplacian u + 0.1*(sum6 - 6u), {N_INTERIOR}^3 interior, "
+                               f"{args.dtype}, zero Dirichlet halo 1 (innermost padded to "
+                               f"{halo[-1]} as compile() aligns), N(0,1) seed 1, one sweep per step",
+                   "grid": list(shape), "temporal_steps": T, "tile": list(r.tile_sizes),
+                   "l2": "arrays 1.15 GB >> 126 MB L2, no flush needed",
+                   "parallelism": f"replicas{world}"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": alg_bytes},
+        "e2e": {"value": round(e2e_gpts, 3), "unit": "GPts/s",
+                "h2d_bytes_per_step": int(u0.nbytes), "d2h_bytes_per_step": int(u0.nbytes),
+                "step": f"H2D of the field, {sweeps} launches of launch_lap7 ({SOLVE_STEPS} steps),"
+                        f" D2H of the result"},
+        "gpu_launches": args.steps,
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return line if rank == 0 else None
+
+
+def _profiled_traffic(dtype: str, T: int):
+    """DRAM bytes per launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "lap7_512_traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    return d.get(f"{dtype}_T{T}")
+
+
+def _slab_job(args):
+    """One worker: time ``steps`` oracle sweeps of a z-slab (seeded)."""
+    nz, dtype_name, steps, seed = args
+    import numpy as np
+
+    import stencil_defs as D
+    from oracle import stencil_oracle as O
+
+    dt = np.dtype(dtype_name)
+    shape = (nz + 2, N_INTERIOR + 2, N_INTERIOR + 2)
+    u = _init_field(shape, (1, 1, 1), dt, seed)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        u = O.apply_stencil(u, D.lap7, 3, (1, 1, 1))
+    return time.perf_counter() - t0, nz * N_INTERIOR * N_INTERIOR * steps
+
+
+def cpu_baseline(np_dtype, cores: int = 1, planes: int = 48, steps: int = 4) -> dict:
+    """The oracle (NumPy restatement of reference/stencil_ref.apply_stencil)
+    on z-slabs of the 512^2 cross-section, ``cores`` worker processes."""
+    import multiprocessing as mp
+
+    import numpy as np
+
+    name = np.dtype(np_dtype).name
+    if cores == 1:
+        secs, pts = _slab_job((planes, name, steps, 0))
+        total_pts, wall = pts, secs
+    else:
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(cores) as pool:
+            pool.map(_slab_job, [(2, name, 1, k) for k in range(cores)])  # warm the workers
+            t0 = time.perf_counter()
+            res = pool.map(_slab_job, [(planes, name, steps, k) for k in range(cores)])
+            wall = time.perf_counter() - t0
+        total_pts = sum(p for _, p in res)
+    return {"value": round(total_pts / wall / 1e9, 5), "unit": "GPts/s", "cores": cores,
+            "kind": "port",
+            "sample": f"{cores} x {steps} sweeps of a {planes}x512x512 z-slab "
+                      f"({name}, oracle apply_stencil, wall {wall:.1f} s)"}
+
+
+def run_reference(args) -> dict | None:
+    import numpy as np
+
+    world, rank, _ = _dist()
+    if rank != 0:
+        return None
+    np_dtype = np.float64 if args.dtype == "float64" else np.float32
+    cores = os.cpu_count() or 1
+    vals = []
+    for k in range(args.warmup + args.steps):
+        cb = cpu_baseline(np_dtype, cores=cores, planes=8, steps=1)
+        if k >= args.warmup:
+            vals.append(cb["value"])
+    value = statistics.median(vals)
+    cb["value"] = value
+    return {
+        "metric": METRIC, "value": value, "unit": "GPts/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(N_INTERIOR ** 3 / (value * 1e9) * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.dtype == "float64" else "f32", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": f"3-D 7-point Laplacian, {N_INTERIOR}^3, {args.dtype}, CPU NumPy "
+                               f"oracle on {cores} processes, z-slab samples"},
+        "cpu_baseline": cb,
+        "e2e": {"value": value, "unit": "GPts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--dtype", choices=("float64", "float32"), default="float64")
+    ap.add_argument("--temporal", type=int, default=1)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    line = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

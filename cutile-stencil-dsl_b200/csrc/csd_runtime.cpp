@@ -1,0 +1,593 @@
+// libcsd: host runtime of the B200 stencil backend.
+//
+// * JIT: NVRTC compiles a generated stencil module for sm_100a; cubins are
+//   cached on disk by a hash of source + headers + options + NVRTC version.
+// * Loading/launching through the CUDA driver API, which is resolved with
+//   dlopen("libcuda.so.1") so the library itself loads on machines without a
+//   GPU driver (CPU-only tests check the exported symbols).
+// * TMA descriptors are encoded per launch with cuTensorMapEncodeTiled.
+//
+// No per-launch allocation: the only device memory this file allocates is
+// one 4-byte error word per device, on first use.
+#include <dlfcn.h>
+#include <nvrtc.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/csd.h"
+
+// ---------------------------------------------------------------------------
+// Minimal driver API surface (types from the CUDA driver API documentation)
+// ---------------------------------------------------------------------------
+typedef int CUresult;
+typedef int CUdevice;
+typedef struct CUctx_st* CUcontext;
+typedef struct CUmod_st* CUmodule;
+typedef struct CUfunc_st* CUfunction;
+typedef struct CUstream_st* CUstream;
+typedef unsigned long long CUdeviceptr;
+
+enum {
+  CU_FUNC_ATTRIBUTE_NUM_REGS_ = 4,
+  CU_FUNC_ATTRIBUTE_LOCAL_SIZE_BYTES_ = 3,
+  CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES_ = 8,
+  CU_DEVICE_ATTRIBUTE_MULTIPROCESSOR_COUNT_ = 16,
+};
+enum {
+  TMAP_FLOAT32 = 7,  // CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+  TMAP_FLOAT64 = 8,  // CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+};
+
+struct Driver {
+  bool ok = false;
+  std::string why;
+  CUresult (*cuInit)(unsigned);
+  CUresult (*cuDeviceGet)(CUdevice*, int);
+  CUresult (*cuDeviceGetAttribute)(int*, int, CUdevice);
+  CUresult (*cuCtxGetCurrent)(CUcontext*);
+  CUresult (*cuCtxSetCurrent)(CUcontext);
+  CUresult (*cuCtxGetDevice)(CUdevice*);
+  CUresult (*cuDevicePrimaryCtxRetain)(CUcontext*, CUdevice);
+  CUresult (*cuModuleLoadData)(CUmodule*, const void*);
+  CUresult (*cuModuleUnload)(CUmodule);
+  CUresult (*cuModuleGetFunction)(CUfunction*, CUmodule, const char*);
+  CUresult (*cuModuleGetGlobal)(CUdeviceptr*, size_t*, CUmodule, const char*);
+  CUresult (*cuMemcpyDtoH)(void*, CUdeviceptr, size_t);
+  CUresult (*cuMemcpyHtoD)(CUdeviceptr, const void*, size_t);
+  CUresult (*cuMemAlloc)(CUdeviceptr*, size_t);
+  CUresult (*cuFuncSetAttribute)(CUfunction, int, int);
+  CUresult (*cuFuncGetAttribute)(int*, int, CUfunction);
+  CUresult (*cuOccupancyMaxActiveBlocksPerMultiprocessor)(int*, CUfunction, int, size_t);
+  CUresult (*cuLaunchKernel)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned,
+                             unsigned, CUstream, void**, void**);
+  CUresult (*cuTensorMapEncodeTiled)(void*, int, unsigned, void*, const unsigned long long*,
+                                     const unsigned long long*, const unsigned*, const unsigned*,
+                                     int, int, int, int);
+  CUresult (*cuGetErrorString)(CUresult, const char**);
+  CUresult (*cuCtxSynchronize)(void);
+};
+
+static thread_local std::string g_last_error;
+static std::mutex g_mu;
+
+static int fail(int code, const char* fmt, ...) {
+  char buf[2048];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+static void load_driver(Driver& d);
+
+static Driver& drv() {
+  static Driver d;
+  static std::once_flag once;
+  std::call_once(once, [] { load_driver(d); });
+  return d;
+}
+
+static void load_driver(Driver& d) {
+  void* h = dlopen("libcuda.so.1", RTLD_NOW | RTLD_GLOBAL);
+  if (!h) h = dlopen("libcuda.so", RTLD_NOW | RTLD_GLOBAL);
+  if (!h) {
+    d.why = "libcuda.so.1 not found (no NVIDIA driver)";
+    return;
+  }
+#define CSD_SYM(field, name)                                                    \
+  d.field = reinterpret_cast<decltype(d.field)>(dlsym(h, name));                \
+  if (!d.field) {                                                               \
+    d.why = std::string("driver symbol missing: ") + name;                      \
+    return;                                                                     \
+  }
+  CSD_SYM(cuInit, "cuInit");
+  CSD_SYM(cuDeviceGet, "cuDeviceGet");
+  CSD_SYM(cuDeviceGetAttribute, "cuDeviceGetAttribute");
+  CSD_SYM(cuCtxGetCurrent, "cuCtxGetCurrent");
+  CSD_SYM(cuCtxSetCurrent, "cuCtxSetCurrent");
+  CSD_SYM(cuCtxGetDevice, "cuCtxGetDevice");
+  CSD_SYM(cuDevicePrimaryCtxRetain, "cuDevicePrimaryCtxRetain");
+  CSD_SYM(cuModuleLoadData, "cuModuleLoadData");
+  CSD_SYM(cuModuleUnload, "cuModuleUnload");
+  CSD_SYM(cuModuleGetFunction, "cuModuleGetFunction");
+  CSD_SYM(cuModuleGetGlobal, "cuModuleGetGlobal_v2");
+  CSD_SYM(cuMemcpyDtoH, "cuMemcpyDtoH_v2");
+  CSD_SYM(cuMemcpyHtoD, "cuMemcpyHtoD_v2");
+  CSD_SYM(cuMemAlloc, "cuMemAlloc_v2");
+  CSD_SYM(cuFuncSetAttribute, "cuFuncSetAttribute");
+  CSD_SYM(cuFuncGetAttribute, "cuFuncGetAttribute");
+  CSD_SYM(cuOccupancyMaxActiveBlocksPerMultiprocessor, "cuOccupancyMaxActiveBlocksPerMultiprocessor");
+  CSD_SYM(cuLaunchKernel, "cuLaunchKernel");
+  CSD_SYM(cuTensorMapEncodeTiled, "cuTensorMapEncodeTiled");
+  CSD_SYM(cuGetErrorString, "cuGetErrorString");
+  CSD_SYM(cuCtxSynchronize, "cuCtxSynchronize");
+#undef CSD_SYM
+  if (d.cuInit(0) != 0) {
+    d.why = "cuInit failed (no usable device)";
+    return;
+  }
+  d.ok = true;
+}
+
+static int cu_fail(CUresult r, const char* what) {
+  const char* s = "unknown";
+  if (drv().cuGetErrorString) drv().cuGetErrorString(r, &s);
+  return fail(CSD_ELAUNCH, "%s failed: CUDA error %d (%s)", what, r, s ? s : "?");
+}
+
+// Make sure a context is current (torch normally made the primary one current).
+static int ensure_context(CUdevice* dev_out) {
+  Driver& d = drv();
+  if (!d.ok) return fail(CSD_ENODEV, "%s", d.why.c_str());
+  CUcontext ctx = nullptr;
+  d.cuCtxGetCurrent(&ctx);
+  if (!ctx) {
+    CUdevice dev;
+    CUresult r = d.cuDeviceGet(&dev, 0);
+    if (r) return cu_fail(r, "cuDeviceGet");
+    r = d.cuDevicePrimaryCtxRetain(&ctx, dev);
+    if (r) return cu_fail(r, "cuDevicePrimaryCtxRetain");
+    r = d.cuCtxSetCurrent(ctx);
+    if (r) return cu_fail(r, "cuCtxSetCurrent");
+  }
+  CUdevice dev;
+  CUresult r = d.cuCtxGetDevice(&dev);
+  if (r) return cu_fail(r, "cuCtxGetDevice");
+  if (dev_out) *dev_out = dev;
+  return CSD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Per-device state: SM count and the error word
+// ---------------------------------------------------------------------------
+struct DeviceState {
+  int sms = 0;
+  CUdeviceptr err = 0;
+};
+static std::unordered_map<int, DeviceState> g_devices;
+
+static int device_state(CUdevice dev, DeviceState** out) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  DeviceState& st = g_devices[dev];
+  if (st.sms == 0) {
+    CUresult r = drv().cuDeviceGetAttribute(&st.sms, CU_DEVICE_ATTRIBUTE_MULTIPROCESSOR_COUNT_, dev);
+    if (r) return cu_fail(r, "cuDeviceGetAttribute");
+  }
+  if (st.err == 0) {
+    CUresult r = drv().cuMemAlloc(&st.err, 16);
+    if (r) return cu_fail(r, "cuMemAlloc(error word)");
+    int zero[4] = {0, 0, 0, 0};
+    r = drv().cuMemcpyHtoD(st.err, zero, sizeof(zero));
+    if (r) return cu_fail(r, "cuMemcpyHtoD(error word)");
+  }
+  *out = &st;
+  return CSD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// JIT compile with a disk cache
+// ---------------------------------------------------------------------------
+static unsigned long long fnv1a(const std::string& s, unsigned long long h = 1469598103934665603ull) {
+  for (unsigned char c : s) {
+    h ^= c;
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+static std::vector<std::string> split_opts(const char* options) {
+  std::vector<std::string> v;
+  if (!options) return v;
+  std::string cur;
+  for (const char* p = options; *p; ++p) {
+    if (*p == '\n') {
+      if (!cur.empty()) v.push_back(cur);
+      cur.clear();
+    } else {
+      cur += *p;
+    }
+  }
+  if (!cur.empty()) v.push_back(cur);
+  return v;
+}
+
+static bool read_file(const std::string& path, std::string* out) {
+  std::ifstream f(path, std::ios::binary);
+  if (!f) return false;
+  std::stringstream ss;
+  ss << f.rdbuf();
+  *out = ss.str();
+  return true;
+}
+
+static int jit_compile(const char* src, int n_headers, const char* const* headers,
+                       const char* const* header_names, const char* options, const char* cache_dir,
+                       std::string* cubin, std::string* path_out, std::string* log_out) {
+  if (!src) return fail(CSD_EINVAL, "null source");
+  int major = 0, minor = 0;
+  nvrtcVersion(&major, &minor);
+  std::string key = src;
+  for (int i = 0; i < n_headers; ++i) {
+    key += "\n//header:";
+    key += header_names[i];
+    key += "\n";
+    key += headers[i];
+  }
+  key += "\n//opts:";
+  key += options ? options : "";
+  key += "\n//nvrtc:" + std::to_string(major) + "." + std::to_string(minor);
+  char hex[32];
+  snprintf(hex, sizeof(hex), "%016llx", fnv1a(key));
+  std::string path;
+  if (cache_dir && *cache_dir) {
+    mkdir(cache_dir, 0755);
+    path = std::string(cache_dir) + "/" + hex + ".cubin";
+    std::string logpath = std::string(cache_dir) + "/" + hex + ".log";
+    if (read_file(path, cubin) && !cubin->empty()) {
+      if (path_out) *path_out = path;
+      if (log_out) read_file(logpath, log_out);
+      return CSD_OK;
+    }
+  }
+  nvrtcProgram prog;
+  nvrtcResult rr = nvrtcCreateProgram(&prog, src, "stencil.cu", n_headers, headers, header_names);
+  if (rr != NVRTC_SUCCESS) return fail(CSD_ECOMPILE, "nvrtcCreateProgram: %s", nvrtcGetErrorString(rr));
+  std::vector<std::string> opts = split_opts(options);
+  std::vector<const char*> argv;
+  for (auto& o : opts) argv.push_back(o.c_str());
+  rr = nvrtcCompileProgram(prog, (int)argv.size(), argv.data());
+  size_t log_size = 0;
+  nvrtcGetProgramLogSize(prog, &log_size);
+  std::string log(log_size, '\0');
+  if (log_size) nvrtcGetProgramLog(prog, &log[0]);
+  log.resize(strlen(log.c_str()));  // drop the terminating NUL
+  if (log_out) *log_out = log;
+  if (rr != NVRTC_SUCCESS) {
+    nvrtcDestroyProgram(&prog);
+    return fail(CSD_ECOMPILE, "NVRTC compilation failed: %s\n%s", nvrtcGetErrorString(rr), log.c_str());
+  }
+  size_t n = 0;
+  rr = nvrtcGetCUBINSize(prog, &n);
+  if (rr != NVRTC_SUCCESS || n == 0) {
+    nvrtcDestroyProgram(&prog);
+    return fail(CSD_ECOMPILE, "nvrtcGetCUBINSize: %s (use a real sm_XXa architecture)",
+                nvrtcGetErrorString(rr));
+  }
+  cubin->assign(n, '\0');
+  nvrtcGetCUBIN(prog, &(*cubin)[0]);
+  nvrtcDestroyProgram(&prog);
+  if (!path.empty()) {
+    std::string tmp = path + ".tmp" + std::to_string(getpid());
+    {
+      std::ofstream f(tmp, std::ios::binary);
+      f.write(cubin->data(), (std::streamsize)cubin->size());
+    }
+    rename(tmp.c_str(), path.c_str());
+    std::ofstream lf(std::string(cache_dir) + "/" + hex + ".log");
+    lf << log;
+    if (path_out) *path_out = path;
+  }
+  return CSD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Modules and kernels
+// ---------------------------------------------------------------------------
+struct csd_module {
+  CUmodule mod = nullptr;
+  CUdevice dev = 0;
+};
+
+struct csd_kernel {
+  csd_module* module = nullptr;
+  CUfunction fn[2] = {nullptr, nullptr};  // [CSD_LOADER_TMA], [CSD_LOADER_LDG]
+  csd_kernel_desc desc;
+  int blocks_per_sm[2] = {0, 0};
+  std::string name;
+};
+
+extern "C" {
+
+int csd_internal_fail(int code, const char* msg) { return fail(code, "%s", msg); }
+
+int csd_version(void) { return 100; }
+
+const char* csd_last_error(void) { return g_last_error.c_str(); }
+
+int csd_compile(const char* src, int n_headers, const char* const* headers,
+                const char* const* header_names, const char* options, const char* cache_dir,
+                char* cubin_path, size_t path_len, char* log, size_t log_len) {
+  std::string cubin, path, lg;
+  int rc = jit_compile(src, n_headers, headers, header_names, options, cache_dir, &cubin, &path, &lg);
+  if (cubin_path && path_len) {
+    snprintf(cubin_path, path_len, "%s", path.c_str());
+  }
+  if (log && log_len) snprintf(log, log_len, "%s", lg.c_str());
+  return rc;
+}
+
+int csd_module_load(const char* src, int n_headers, const char* const* headers,
+                    const char* const* header_names, const char* options, const char* cache_dir,
+                    csd_module** out) {
+  if (!out) return fail(CSD_EINVAL, "null output handle");
+  CUdevice dev;
+  int rc = ensure_context(&dev);
+  if (rc) return rc;
+  std::string cubin, path, log;
+  rc = jit_compile(src, n_headers, headers, header_names, options, cache_dir, &cubin, &path, &log);
+  if (rc) return rc;
+  CUmodule mod;
+  CUresult r = drv().cuModuleLoadData(&mod, cubin.data());
+  if (r) return cu_fail(r, "cuModuleLoadData");
+  csd_module* m = new csd_module();
+  m->mod = mod;
+  m->dev = dev;
+  *out = m;
+  return CSD_OK;
+}
+
+int csd_module_unload(csd_module* m) {
+  if (!m) return CSD_OK;
+  if (m->mod && drv().ok) drv().cuModuleUnload(m->mod);
+  delete m;
+  return CSD_OK;
+}
+
+int csd_kernel_get(csd_module* m, const char* name, csd_kernel** out) {
+  if (!m || !name || !out) return fail(CSD_EINVAL, "null argument");
+  Driver& d = drv();
+  csd_kernel* k = new csd_kernel();
+  k->module = m;
+  k->name = name;
+  std::string n = name;
+  CUresult r = d.cuModuleGetFunction(&k->fn[CSD_LOADER_TMA], m->mod, (n + "_tma").c_str());
+  if (r) {
+    delete k;
+    return fail(CSD_ENOSYM, "kernel %s_tma not found in module", name);
+  }
+  r = d.cuModuleGetFunction(&k->fn[CSD_LOADER_LDG], m->mod, (n + "_ldg").c_str());
+  if (r) {
+    delete k;
+    return fail(CSD_ENOSYM, "kernel %s_ldg not found in module", name);
+  }
+  CUdeviceptr dp;
+  size_t sz;
+  r = d.cuModuleGetGlobal(&dp, &sz, m->mod, (n + "_desc").c_str());
+  if (r || sz != sizeof(csd_kernel_desc)) {
+    delete k;
+    return fail(CSD_ENOSYM, "descriptor %s_desc not found (size %zu)", name, (size_t)sz);
+  }
+  r = d.cuMemcpyDtoH(&k->desc, dp, sizeof(csd_kernel_desc));
+  if (r) {
+    delete k;
+    return cu_fail(r, "cuMemcpyDtoH(desc)");
+  }
+  if (k->desc.magic != CSD_DESC_MAGIC) {
+    delete k;
+    return fail(CSD_ENOSYM, "bad descriptor magic for %s", name);
+  }
+  for (int l = 0; l < 2; ++l) {
+    r = d.cuFuncSetAttribute(k->fn[l], CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES_,
+                             k->desc.smem_bytes);
+    if (r) {
+      delete k;
+      return cu_fail(r, "cuFuncSetAttribute(max dynamic smem)");
+    }
+    r = d.cuOccupancyMaxActiveBlocksPerMultiprocessor(&k->blocks_per_sm[l], k->fn[l],
+                                                      k->desc.threads, (size_t)k->desc.smem_bytes);
+    if (r) {
+      delete k;
+      return cu_fail(r, "cuOccupancyMaxActiveBlocksPerMultiprocessor");
+    }
+    if (k->blocks_per_sm[l] < 1) k->blocks_per_sm[l] = 1;
+  }
+  *out = k;
+  return CSD_OK;
+}
+
+int csd_kernel_describe(const csd_kernel* k, csd_kernel_desc* out) {
+  if (!k || !out) return fail(CSD_EINVAL, "null argument");
+  *out = k->desc;
+  return CSD_OK;
+}
+
+int csd_kernel_resources(csd_kernel* k, int* regs, int* local_bytes, int* blocks_per_sm) {
+  if (!k) return fail(CSD_EINVAL, "null kernel");
+  Driver& d = drv();
+  if (regs) d.cuFuncGetAttribute(regs, CU_FUNC_ATTRIBUTE_NUM_REGS_, k->fn[CSD_LOADER_TMA]);
+  if (local_bytes) d.cuFuncGetAttribute(local_bytes, CU_FUNC_ATTRIBUTE_LOCAL_SIZE_BYTES_, k->fn[CSD_LOADER_TMA]);
+  if (blocks_per_sm) *blocks_per_sm = k->blocks_per_sm[CSD_LOADER_TMA];
+  return CSD_OK;
+}
+
+// Map an N-D array (halo included) to the engine's (Z, Y, X) view.
+static void view3(const csd_field& f, long long dims[3], const int halo_in[3], int halo[3]) {
+  if (f.ndim == 3) {
+    for (int i = 0; i < 3; ++i) {
+      dims[i] = f.shape[i];
+      halo[i] = halo_in[i];
+    }
+  } else if (f.ndim == 2) {
+    dims[0] = f.shape[0];
+    dims[1] = 1;
+    dims[2] = f.shape[1];
+    halo[0] = halo_in[0];
+    halo[1] = 0;
+    halo[2] = halo_in[1];
+  } else {
+    dims[0] = 1;
+    dims[1] = 1;
+    dims[2] = f.shape[0];
+    halo[0] = 0;
+    halo[1] = 0;
+    halo[2] = halo_in[0];
+  }
+}
+
+static bool contiguous(const csd_field& f) {
+  long long expect = 1;
+  for (int i = f.ndim - 1; i >= 0; --i) {
+    if (f.shape[i] != 1 && f.strides[i] != expect) return false;
+    expect *= f.shape[i];
+  }
+  return true;
+}
+
+int csd_launch(csd_kernel* k, const csd_field* in, int n_in, const csd_field* out, int n_out,
+               const csd_launch_opts* opts, void* stream) {
+  if (!k || !in || !out) return fail(CSD_EINVAL, "null argument");
+  const csd_kernel_desc& D = k->desc;
+  if (n_in != D.nin || n_out != D.nout)
+    return fail(CSD_EINVAL, "kernel %s takes %d inputs and %d outputs, got %d and %d",
+                k->name.c_str(), D.nin, D.nout, n_in, n_out);
+  if (n_in > CSD_MAX_FIELDS || n_out > CSD_MAX_FIELDS) return fail(CSD_EINVAL, "too many fields");
+  const csd_field& f0 = in[0];
+  if (f0.ndim != D.ndim) return fail(CSD_EINVAL, "kernel is %d-D, array is %d-D", D.ndim, f0.ndim);
+  const int want_dtype = D.dtype_bytes == 8 ? CSD_DTYPE_F64 : CSD_DTYPE_F32;
+  for (int i = 0; i < n_in + n_out; ++i) {
+    const csd_field& f = i < n_in ? in[i] : out[i - n_in];
+    if (f.ndim != f0.ndim) return fail(CSD_EINVAL, "all fields must have the same ndim");
+    for (int d = 0; d < f.ndim; ++d)
+      if (f.shape[d] != f0.shape[d]) return fail(CSD_EINVAL, "all fields must have the same shape");
+    if (f.dtype != want_dtype) return fail(CSD_EINVAL, "field dtype does not match the kernel");
+    if (!contiguous(f)) return fail(CSD_EINVAL, "fields must be C-contiguous");
+    if (!f.ptr) return fail(CSD_EINVAL, "null field pointer");
+    if ((reinterpret_cast<uintptr_t>(f.ptr) % D.dtype_bytes) != 0)
+      return fail(CSD_EALIGN, "field pointer not aligned to its element size");
+  }
+  csd_launch_opts o = {};
+  if (opts) o = *opts;
+  CUdevice dev;
+  int rc = ensure_context(&dev);
+  if (rc) return rc;
+  DeviceState* st;
+  rc = device_state(dev, &st);
+  if (rc) return rc;
+
+  csd_params p;
+  memset(&p, 0, sizeof(p));
+  int halo[3];
+  view3(f0, p.dims, o.halo, halo);
+  const int rad[3] = {D.rz, D.ry, D.rx};
+  for (int d = 0; d < 3; ++d) {
+    p.halo[d] = halo[d];
+    p.interior[d] = (int)(p.dims[d] - 2 * halo[d]);
+    if (p.interior[d] <= 0 && p.dims[d] > 0)
+      return fail(CSD_EINVAL, "array extent %lld leaves no interior with halo %d", p.dims[d], halo[d]);
+    if (halo[d] < rad[d])
+      return fail(CSD_EINVAL, "array halo %d is smaller than the stencil radius %d", halo[d], rad[d]);
+  }
+  p.pitch_y = p.dims[2];
+  p.pitch_z = p.dims[1] * p.dims[2];
+  for (int i = 0; i < n_in; ++i) p.in[i] = in[i].ptr;
+  for (int i = 0; i < n_out; ++i) p.out[i] = out[i].ptr;
+  p.xbase = (p.halo[2] / D.align) * D.align;
+  p.tiles[0] = (p.halo[2] + p.interior[2] - p.xbase + D.tile_x - 1) / D.tile_x;
+  p.tiles[1] = (p.interior[1] + D.tile_y - 1) / D.tile_y;
+  p.zchunk = o.zchunk > 0 ? o.zchunk : D.zchunk;
+  p.zchunk = ((p.zchunk + D.rows - 1) / D.rows) * D.rows;
+  if (p.zchunk > p.interior[0]) p.zchunk = ((p.interior[0] + D.rows - 1) / D.rows) * D.rows;
+  p.tiles[2] = (p.interior[0] + p.zchunk - 1) / p.zchunk;
+  long long items = (long long)p.tiles[0] * p.tiles[1] * p.tiles[2];
+  if (items > 0x7fffffff) return fail(CSD_EINVAL, "too many work items");
+  p.items = (int)items;
+  p.bc_mode = D.bc_mode;
+  p.bc_value = o.bc_value;
+  p.err = reinterpret_cast<int*>(st->err);
+  p.timeout_ns = o.timeout_ns ? o.timeout_ns : 2000000000ull;
+  const long long esz = D.dtype_bytes;
+  bool vec = true;
+  for (int i = 0; i < n_out; ++i) vec = vec && (reinterpret_cast<uintptr_t>(out[i].ptr) % 16 == 0);
+  vec = vec && ((p.pitch_y * esz) % 16 == 0) && ((p.pitch_z * esz) % 16 == 0);
+  p.vec_store = vec ? 1 : 0;
+
+  // Loader: TMA when every input is 16-byte aligned with 16-byte pitches.
+  bool tma_ok = ((p.dims[2] * esz) % 16 == 0) && ((p.pitch_z * esz) % 16 == 0);
+  for (int i = 0; i < n_in; ++i) tma_ok = tma_ok && (reinterpret_cast<uintptr_t>(in[i].ptr) % 16 == 0);
+  int loader = o.loader;
+  if (loader < 0 || loader > 1) loader = tma_ok ? CSD_LOADER_TMA : CSD_LOADER_LDG;
+  if (loader == CSD_LOADER_TMA && !tma_ok)
+    return fail(CSD_EALIGN, "TMA path needs 16-byte aligned fields and row pitch");
+  if (loader == CSD_LOADER_TMA) {
+    Driver& d = drv();
+    for (int i = 0; i < n_in; ++i) {
+      unsigned long long gdim[3] = {(unsigned long long)p.dims[2], (unsigned long long)p.dims[1],
+                                    (unsigned long long)p.dims[0]};
+      unsigned long long gstride[2] = {(unsigned long long)(p.pitch_y * esz),
+                                       (unsigned long long)(p.pitch_z * esz)};
+      unsigned box[3] = {(unsigned)D.box_w, (unsigned)D.box_h, (unsigned)D.rows};
+      unsigned estride[3] = {1, 1, 1};
+      CUresult r = d.cuTensorMapEncodeTiled(&p.tmap[i], esz == 8 ? TMAP_FLOAT64 : TMAP_FLOAT32, 3,
+                                            in[i].ptr, gdim, gstride, box, estride,
+                                            0 /*interleave none*/, 0 /*swizzle none*/,
+                                            2 /*L2 promotion 128B*/, 0 /*OOB fill zeros*/);
+      if (r) return cu_fail(r, "cuTensorMapEncodeTiled");
+    }
+  }
+  int grid = o.grid > 0 ? o.grid : k->blocks_per_sm[loader] * st->sms;
+  if (grid > p.items) grid = p.items;
+  if (grid < 1) return CSD_OK;  // nothing to do
+  void* args[] = {&p};
+  CUresult r = drv().cuLaunchKernel(k->fn[loader], (unsigned)grid, 1, 1, (unsigned)D.threads, 1, 1,
+                                    (unsigned)D.smem_bytes, reinterpret_cast<CUstream>(stream), args,
+                                    nullptr);
+  if (r) return cu_fail(r, "cuLaunchKernel");
+  return CSD_OK;
+}
+
+int csd_error_word(int* value, int reset) {
+  CUdevice dev;
+  int rc = ensure_context(&dev);
+  if (rc) return rc;
+  DeviceState* st;
+  rc = device_state(dev, &st);
+  if (rc) return rc;
+  Driver& d = drv();
+  CUresult r = d.cuCtxSynchronize();
+  if (r) return cu_fail(r, "cuCtxSynchronize");
+  int v = 0;
+  r = d.cuMemcpyDtoH(&v, st->err, sizeof(int));
+  if (r) return cu_fail(r, "cuMemcpyDtoH(error word)");
+  if (value) *value = v;
+  if (reset && v) {
+    int zero = 0;
+    r = d.cuMemcpyHtoD(st->err, &zero, sizeof(int));
+    if (r) return cu_fail(r, "cuMemcpyHtoD(error word)");
+  }
+  return CSD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,454 @@
+// Streaming stencil engine for sm_100a.
+//
+// A work item is a column of TY x TX points (internal dims Y, X) that walks
+// ZCHUNK output rows of Z, ROWS rows per step.  Input rows reach shared
+// memory as chunks of ROWS x BOXH x BOXW elements (the tile plus the
+// stencil halo, X padded to 16-byte boundaries), either as one TMA tile
+// copy per field per chunk (cp.async.bulk.tensor, completion counted on an
+// mbarrier) or, when the array pitch is not 16-byte aligned, as per-element
+// cp.async copies arriving on the same mbarrier.  Chunks live in a ring of
+// NSLOT slots: 2*HC+1 are read by the current step, STAGES more are in
+// flight.  Work items are handed out round-robin to a persistent grid.
+//
+// With TEMPORAL = T > 1 one pass chains T stencil steps (time skewing): at
+// ring step i, stage s computes chunk i - s*HC of the s-th intermediate field
+// into its own shared-memory ring (which is (T-s)*radius wider than the
+// tile), and stage T writes the final field.  Intermediate points outside the
+// domain interior are zero, which is what T separate launches through
+// zero-halo scratch buffers produce.
+//
+// The stencil body is a functor emitted from the DSL: it reads "strips"
+// (a row segment of one field at a Z/Y offset) through the tile view and
+// evaluates each point with round-to-nearest intrinsics in DSL term order.
+#ifndef CSD_ENGINE_CUH
+#define CSD_ENGINE_CUH
+
+#include "csd/params.h"
+#include "csd/ptx.cuh"
+
+namespace csd {
+
+template <typename T>
+struct VecOf;
+template <>
+struct VecOf<double> {
+  typedef double2 type;
+  static constexpr int N = 2;
+};
+template <>
+struct VecOf<float> {
+  typedef float4 type;
+  static constexpr int N = 4;
+};
+
+__host__ __device__ constexpr int cdiv(int a, int b) { return (a + b - 1) / b; }
+__host__ __device__ constexpr int align_up(int a, int b) { return cdiv(a, b) * b; }
+// floor division for possibly negative numerators (b > 0)
+__host__ __device__ constexpr int fdiv(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
+__host__ __device__ constexpr int imax(int a, int b) { return a > b ? a : b; }
+
+// ---------------------------------------------------------------------------
+// Compile-time configuration
+// ---------------------------------------------------------------------------
+template <typename T_, int NIN_, int NOUT_, int RZ_, int RY_, int RX_, int ROWS_, int TY_, int TX_,
+          int NT_, int STAGES_, int TEMPORAL_, int LOADER_, int BC_>
+struct Cfg {
+  typedef T_ T;
+  static constexpr int NIN = NIN_, NOUT = NOUT_;
+  static constexpr int RZ = RZ_, RY = RY_, RX = RX_;  // radius of ONE step
+  static constexpr int ROWS = ROWS_, TY = TY_, TX = TX_;
+  static constexpr int NT = NT_, STAGES = STAGES_, TEMPORAL = TEMPORAL_;
+  static constexpr int LOADER = LOADER_, BC = BC_;
+  static constexpr int ALIGN = 16 / (int)sizeof(T);
+  static constexpr int VEC = ALIGN;
+  static constexpr int HC = RZ > 0 ? cdiv(RZ, ROWS) : 0;  // halo chunks per side, per step
+  // Column layout shared by every buffer: smem column c <-> x = X0 - PADL + c.
+  static constexpr int RXA = align_up(RX, ALIGN);
+  static constexpr int PADL = TEMPORAL == 1 ? RXA : align_up(TEMPORAL * RX + 2 * ALIGN - 2, ALIGN);
+  static constexpr int BOXW = TEMPORAL == 1 ? align_up(PADL + TX + RX, ALIGN)
+                                            : align_up(PADL + TX + TEMPORAL * RX + 2 * ALIGN - 2, ALIGN);
+  // Height (Y rows) of the buffer holding the field after s steps.
+  static __host__ __device__ constexpr int H(int s) { return TY + 2 * (TEMPORAL - s) * RY; }
+  static constexpr int BOXH = TY + 2 * TEMPORAL * RY;
+  static constexpr int NSLOT = 2 * HC + 1 + STAGES;              // input ring
+  static constexpr int NSLOT_I = 2 * HC + 1;                     // intermediate rings
+  static constexpr int SLOT_ELEMS = align_up(ROWS * BOXH * BOXW, 128 / (int)sizeof(T));
+  static constexpr int CHUNK_BYTES = ROWS * BOXH * BOXW * (int)sizeof(T);  // TMA bytes
+  static __host__ __device__ constexpr int ISLOT_ELEMS(int s) {
+    return align_up(ROWS * H(s) * BOXW, 128 / (int)sizeof(T));
+  }
+  static __host__ __device__ constexpr int inter_elems_upto(int s) {  // rings 1..s-1
+    return s <= 1 ? 0 : inter_elems_upto(s - 1) + NSLOT_I * ISLOT_ELEMS(s - 1);
+  }
+  static constexpr int RING_ELEMS = NIN * NSLOT * SLOT_ELEMS;
+  static constexpr int INTER_ELEMS = inter_elems_upto(TEMPORAL);
+  static constexpr int BAR_OFFSET = (RING_ELEMS + INTER_ELEMS) * (int)sizeof(T);
+  // +128: the dynamic shared-memory base is aligned up to 128 bytes in the kernel
+  static constexpr int SMEM_BYTES = BAR_OFFSET + 8 * NSLOT + 64 + 128;
+  static_assert(BOXW <= 256 && BOXH <= 256 && ROWS <= 256, "TMA box limit");
+  static_assert(TX % VEC == 0, "tile width must be a multiple of the vector width");
+  static_assert(TEMPORAL == 1 || (NIN == 1 && NOUT == 1), "temporal chains need one field");
+  static_assert(HC * ROWS >= RZ, "halo chunks");
+  static_assert(BC == CSD_BC_NONE || TEMPORAL == 1, "fused boundary fill is single-step");
+};
+
+// ---------------------------------------------------------------------------
+// Strips: VEC consecutive points' worth of one row segment [LO, VEC-1+HI]
+// ---------------------------------------------------------------------------
+template <typename T, int LO, int HI, int VEC>
+struct Strip {
+  T v[VEC + HI - LO];
+};
+
+template <typename T, int LO, int HI, int VEC, int ALIGN>
+__device__ __forceinline__ Strip<T, LO, HI, VEC> load_strip(const T* row, int x) {
+  // row: smem row base; x: column of the unit's first point (multiple of ALIGN)
+  constexpr int A0 = fdiv(LO, ALIGN) * ALIGN;             // aligned start offset
+  constexpr int A1 = align_up(VEC + HI, ALIGN);            // aligned end offset (exclusive)
+  constexpr int NV = (A1 - A0) / ALIGN;
+  typedef typename VecOf<T>::type V;
+  T buf[NV * ALIGN];
+  const V* src = reinterpret_cast<const V*>(row + x + A0);
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    const V t = src[i];
+    *reinterpret_cast<V*>(&buf[i * ALIGN]) = t;
+  }
+  Strip<T, LO, HI, VEC> s;
+#pragma unroll
+  for (int i = 0; i < VEC + HI - LO; ++i) s.v[i] = buf[i + (LO - A0)];
+  return s;
+}
+
+// View of one buffer (ring of chunks) for the body functor.
+template <class C>
+struct TileView {
+  typedef typename C::T T;
+  const T* base[C::NIN];  // per-field ring base
+  int slot0;              // slot of the step's first source chunk
+  int nslot;              // slots in the ring
+  int slot_elems;
+  int height;             // Y rows per chunk row
+  int y_off;              // buffer row of the unit's y (source has extra halo rows)
+
+  // Row segment of field F at Z offset DZ and Y offset DY for unit (r, y, x).
+  template <int F, int DZ, int DY, int LO, int HI>
+  __device__ __forceinline__ Strip<T, LO, HI, C::VEC> strip(int r, int y, int x) const {
+    const int q = C::HC * C::ROWS + r + DZ;  // >= 0
+    const int c = q / C::ROWS;
+    const int rr = q - c * C::ROWS;
+    int slot = slot0 + c;
+    if (slot >= nslot) slot -= nslot;
+    const T* row = base[F] + slot * slot_elems + (rr * height + (y + y_off + DY)) * C::BOXW;
+    return load_strip<T, LO, HI, C::VEC, C::ALIGN>(row, x);
+  }
+};
+
+// Output value pack for one unit.
+template <typename T, int NOUT, int VEC>
+struct OutPack {
+  T v[NOUT][VEC];
+};
+
+__device__ __forceinline__ void store_vec(double* p, const double* v) {
+  *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+}
+__device__ __forceinline__ void store_vec(float* p, const float* v) {
+  *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+
+// Fused boundary fill: map an out-of-interior index of one dim to the
+// interior index whose value it takes (periodic / Neumann / reflecting), as
+// apply_boundary does with its slab copies.  Dirichlet is handled by value.
+__device__ __forceinline__ long long bc_map(long long i, int h, int n, int mode) {
+  if (i >= h && i < h + n) return i;
+  if (mode == CSD_BC_PERIODIC) {
+    long long k = (i - h) % n;
+    if (k < 0) k += n;
+    return h + k;
+  }
+  if (mode == CSD_BC_NEUMANN) return i < h ? h : h + n - 1;
+  // reflecting: index h-1-k <- h+k, h+n+k <- h+n-1-k
+  if (i < h) return 2 * h - 1 - i;
+  return 2 * (h + n) - 1 - i;
+}
+
+// ---------------------------------------------------------------------------
+// Chunk loaders
+// ---------------------------------------------------------------------------
+template <class C>
+struct Loader {
+  typedef typename C::T T;
+
+  // Issue the copies of one chunk (all fields) into `slot`.
+  static __device__ __forceinline__ void issue(const csd_params& p, T* ring, unsigned bar,
+                                               int slot, int x0, int y0, int z0) {
+    if constexpr (C::LOADER == CSD_LOADER_TMA) {
+      if (threadIdx.x == 0) {
+        ptx::mbar_arrive_expect_tx(bar, (unsigned)(C::CHUNK_BYTES * C::NIN));
+#pragma unroll
+        for (int f = 0; f < C::NIN; ++f) {
+          T* dst = ring + (f * C::NSLOT + slot) * C::SLOT_ELEMS;
+          ptx::tma_load_3d(ptx::smem_addr(dst), &p.tmap[f], x0, y0, z0, bar);
+        }
+      }
+    } else {
+      constexpr int N = C::ROWS * C::BOXH * C::BOXW;
+      const long long NZ = p.dims[0], NY = p.dims[1], NX = p.dims[2];
+#pragma unroll 1
+      for (int e = threadIdx.x; e < N; e += C::NT) {
+        const int xx = e % C::BOXW;
+        const int t = e / C::BOXW;
+        const int yy = t % C::BOXH;
+        const int rr = t / C::BOXH;
+        const long long gx = (long long)x0 + xx, gy = (long long)y0 + yy, gz = (long long)z0 + rr;
+        const bool ok = gx >= 0 && gx < NX && gy >= 0 && gy < NY && gz >= 0 && gz < NZ;
+        const long long off = ok ? (gz * p.pitch_z + gy * p.pitch_y + gx) : 0;
+#pragma unroll
+        for (int f = 0; f < C::NIN; ++f) {
+          T* dst = ring + (f * C::NSLOT + slot) * C::SLOT_ELEMS + e;
+          const T* src = reinterpret_cast<const T*>(p.in[f]) + off;
+          ptx::cp_async_zfill<sizeof(T)>(ptx::smem_addr(dst), src, ok);
+        }
+      }
+      ptx::cp_async_arrive(bar);
+    }
+  }
+};
+
+// Overwrite the cells of a freshly landed chunk that lie outside the domain
+// interior with their boundary-condition values (fused boundary fill).
+template <class C>
+__device__ __forceinline__ void patch_boundary(const csd_params& p, typename C::T* ring, int slot,
+                                               int x0, int y0, int z0) {
+  typedef typename C::T T;
+  const int hz = p.halo[0], hy = p.halo[1], hx = p.halo[2];
+  const int nz = p.interior[0], ny = p.interior[1], nx = p.interior[2];
+  const bool edge = x0 < hx || x0 + C::BOXW > hx + nx || y0 < hy || y0 + C::BOXH > hy + ny ||
+                    z0 < hz || z0 + C::ROWS > hz + nz;
+  if (!edge) return;
+  constexpr int N = C::ROWS * C::BOXH * C::BOXW;
+  for (int e = threadIdx.x; e < N; e += C::NT) {
+    const int xx = e % C::BOXW;
+    const int t = e / C::BOXW;
+    const int yy = t % C::BOXH;
+    const int rr = t / C::BOXH;
+    const long long gx = (long long)x0 + xx, gy = (long long)y0 + yy, gz = (long long)z0 + rr;
+    const bool inside = gx >= hx && gx < hx + nx && gy >= hy && gy < hy + ny && gz >= hz &&
+                        gz < hz + nz;
+    if (inside) continue;
+    // cells beyond the array's own extent are never read by interior points
+    if (gx < 0 || gy < 0 || gz < 0 || gx >= p.dims[2] || gy >= p.dims[1] || gz >= p.dims[0])
+      continue;
+#pragma unroll
+    for (int f = 0; f < C::NIN; ++f) {
+      T v;
+      if (C::BC == CSD_BC_DIRICHLET) {
+        v = (T)p.bc_value;
+      } else {
+        const long long mx = (nx > 0 && p.dims[2] > 1) ? bc_map(gx, hx, nx, C::BC) : gx;
+        const long long my = (ny > 0 && p.dims[1] > 1) ? bc_map(gy, hy, ny, C::BC) : gy;
+        const long long mz = (nz > 0 && p.dims[0] > 1) ? bc_map(gz, hz, nz, C::BC) : gz;
+        v = reinterpret_cast<const T*>(p.in[f])[mz * p.pitch_z + my * p.pitch_y + mx];
+      }
+      ring[(f * C::NSLOT + slot) * C::SLOT_ELEMS + e] = v;
+    }
+  }
+  // the slot will be refilled by TMA (async proxy) after these generic writes
+  ptx::fence_proxy_async_smem();
+}
+
+// ---------------------------------------------------------------------------
+// The engine
+// ---------------------------------------------------------------------------
+template <class C, class Body>
+__device__ __forceinline__ void stream_engine(const csd_params& p) {
+  typedef typename C::T T;
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  // TMA destinations must be 128-byte aligned: align the base explicitly
+  unsigned char* smem_raw = smem_dyn + ((128u - (ptx::smem_addr(smem_dyn) & 127u)) & 127u);
+  T* ring = reinterpret_cast<T*>(smem_raw);
+  T* inter = ring + C::RING_ELEMS;
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem_raw + C::BAR_OFFSET);
+  __shared__ int abort_flag;
+
+  if (threadIdx.x == 0) {
+    abort_flag = 0;
+#pragma unroll 1
+    for (int s = 0; s < C::NSLOT; ++s)
+      ptx::mbar_init(ptx::smem_addr(&bars[s]), C::LOADER == CSD_LOADER_TMA ? 1u : (unsigned)C::NT);
+    ptx::fence_mbar_init();
+  }
+  // Zero the intermediate rings once: rows/columns a stage never writes are
+  // read only by points whose results are discarded, but must not hold NaN
+  // garbage that could be mistaken for data by a debugging reader.
+  for (int e = threadIdx.x; e < C::INTER_ELEMS; e += C::NT) inter[e] = T(0);
+  __syncthreads();
+
+  const int hz = p.halo[0], hy = p.halo[1], hx = p.halo[2];
+  const int nz = p.interior[0], ny = p.interior[1], nx = p.interior[2];
+  constexpr int T_ = C::TEMPORAL;
+  constexpr int HCT = C::HC * T_;  // input halo chunks per side for the whole chain
+  unsigned seq = 0;                // chunks consumed by this CTA so far
+
+  for (int item = blockIdx.x; item < p.items; item += gridDim.x) {
+    const int tx = item % p.tiles[0];
+    const int t1 = item / p.tiles[0];
+    const int ty = t1 % p.tiles[1];
+    const int tz = t1 / p.tiles[1];
+    const int X0 = p.xbase + tx * C::TX;  // array column of the tile's first point
+    const int Y0 = hy + ty * C::TY;
+    const int z0 = tz * p.zchunk;         // interior row of the item's first output row
+    const int nrows = min(p.zchunk, nz - z0);
+    const int nsteps = cdiv(nrows, C::ROWS);
+    const int nchunks = nsteps + 2 * HCT;
+    // array coordinates of input chunk 0
+    const int cx = X0 - C::PADL;
+    const int cy = Y0 - T_ * C::RY;
+    const int cz = hz + z0 - HCT * C::ROWS;
+
+    // prologue: fill the ring
+    const int pre = min(nchunks, C::NSLOT);
+    int issued = pre;   // chunks [0, issued) have been issued
+    int waited = 0;     // chunks [0, waited) have landed
+    for (int k = 0; k < pre; ++k) {
+      const unsigned g = seq + k;
+      const int slot = g % C::NSLOT;
+      Loader<C>::issue(p, ring, ptx::smem_addr(&bars[slot]), slot, cx, cy, cz + k * C::ROWS);
+    }
+
+    for (int i = 0; i < nchunks; ++i) {
+      // wait for input chunk i
+      {
+        const unsigned g = seq + i;
+        const int slot = g % C::NSLOT;
+        const unsigned parity = (g / C::NSLOT) & 1u;
+        if (!ptx::mbar_wait(ptx::smem_addr(&bars[slot]), parity, p.timeout_ns)) {
+          abort_flag = 1;
+          if (p.err) atomicExch(p.err, CSD_ERR_TIMEOUT);
+        }
+        waited = i;
+        if constexpr (C::BC != CSD_BC_NONE) {
+          __syncthreads();
+          if (!abort_flag) patch_boundary<C>(p, ring, slot, cx, cy, cz + i * C::ROWS);
+        }
+      }
+      __syncthreads();
+      if (abort_flag) break;
+
+      // stages 1..T: stage s computes chunk k_s = i - s*HC of its field
+#pragma unroll
+      for (int s = 1; s <= T_; ++s) {
+        const int k = i - s * C::HC;   // chunk index in the common chunk grid
+        const int klo = s * C::HC;     // first chunk of field s that is needed
+        const int khi = nsteps + (2 * T_ - s) * C::HC;  // one past the last
+        if (k < klo || k >= khi) continue;
+        // source: field s-1, chunks k-HC .. k+HC
+        TileView<C> src;
+        const int c0 = k - C::HC;  // first source chunk
+        if (s == 1) {
+#pragma unroll
+          for (int f = 0; f < C::NIN; ++f) src.base[f] = ring + f * C::NSLOT * C::SLOT_ELEMS;
+          src.slot0 = (int)((seq + (unsigned)c0) % C::NSLOT);
+          src.nslot = C::NSLOT;
+          src.slot_elems = C::SLOT_ELEMS;
+        } else {
+          src.base[0] = inter + C::inter_elems_upto(s - 1);
+          src.slot0 = c0 % C::NSLOT_I;
+          src.nslot = C::NSLOT_I;
+          src.slot_elems = C::ISLOT_ELEMS(s - 1);
+        }
+        src.height = C::H(s - 1);
+        src.y_off = C::RY;  // source buffer has RY more rows on each side
+        const int hs = C::H(s);
+        // destination geometry
+        const bool last = (s == T_);
+        int xv_lo, xv_hi;
+        if (last) {
+          xv_lo = C::PADL / C::VEC;
+          xv_hi = (C::PADL + C::TX) / C::VEC;
+        } else {
+          xv_lo = fdiv(C::PADL - (T_ - s) * C::RX, C::VEC);
+          xv_hi = cdiv(C::PADL + C::TX + (T_ - s) * C::RX, C::VEC);
+        }
+        const int nxv = xv_hi - xv_lo;
+        const int units = C::ROWS * hs * nxv;
+        // Z row (interior index) of this chunk's first row for field s
+        const int zrow0 = z0 + (k - HCT) * C::ROWS;
+        const int ybuf0 = Y0 - (T_ - s) * C::RY;  // array row of dst buffer row 0
+        T* dst = last ? nullptr
+                      : inter + C::inter_elems_upto(s) + (k % C::NSLOT_I) * C::ISLOT_ELEMS(s);
+#pragma unroll 1
+        for (int u = threadIdx.x; u < units; u += C::NT) {
+          const int xv = xv_lo + u % nxv;
+          const int t2 = u / nxv;
+          const int y = t2 % hs;
+          const int r = t2 / hs;
+          OutPack<T, C::NOUT, C::VEC> o;
+          Body::template compute<C>(src, r, y, xv * C::VEC, o);
+          const int gz = hz + zrow0 + r;                 // array coordinates
+          const int gy = ybuf0 + y;
+          const int gx0 = X0 - C::PADL + xv * C::VEC;
+          const bool zin = zrow0 + r >= 0 && zrow0 + r < nz;
+          const bool yin = gy >= hy && gy < hy + ny;
+          if (last) {
+            if (!(zin && yin && (zrow0 + r) < z0 + nrows)) continue;
+            const long long rowoff = (long long)gz * p.pitch_z + (long long)gy * p.pitch_y;
+            const bool full = gx0 >= hx && gx0 + C::VEC <= hx + nx;
+#pragma unroll
+            for (int f = 0; f < C::NOUT; ++f) {
+              T* out = reinterpret_cast<T*>(p.out[f]) + rowoff;
+              if (full && p.vec_store) {
+                store_vec(out + gx0, o.v[f]);
+              } else {
+#pragma unroll
+                for (int e = 0; e < C::VEC; ++e) {
+                  const int gx = gx0 + e;
+                  if (gx >= hx && gx < hx + nx) out[gx] = o.v[f][e];
+                }
+              }
+            }
+          } else {
+            T* d = dst + (r * hs + y) * C::BOXW + xv * C::VEC;
+#pragma unroll
+            for (int e = 0; e < C::VEC; ++e) {
+              const int gx = gx0 + e;
+              const bool in = zin && yin && gx >= hx && gx < hx + nx;
+              d[e] = in ? o.v[0][e] : T(0);
+            }
+          }
+        }
+        __syncthreads();
+      }
+
+      // refill: input chunk i - 2*HC is dead, its slot takes chunk i - 2*HC + NSLOT
+      {
+        const int dead = i - 2 * C::HC;
+        if (dead >= 0 && dead + C::NSLOT < nchunks) {
+          const int nk = dead + C::NSLOT;
+          const unsigned g = seq + nk;
+          const int slot = g % C::NSLOT;
+          if (C::LOADER == CSD_LOADER_TMA && threadIdx.x == 0) ptx::fence_proxy_async_smem();
+          Loader<C>::issue(p, ring, ptx::smem_addr(&bars[slot]), slot, cx, cy, cz + nk * C::ROWS);
+          issued = nk + 1;
+        }
+      }
+    }
+    if (abort_flag) {
+      // drain: wait (bounded) for the copies still in flight before leaving
+      if (threadIdx.x == 0) {
+        for (int k = waited; k < issued; ++k) {
+          const unsigned g = seq + k;
+          ptx::mbar_wait(ptx::smem_addr(&bars[g % C::NSLOT]), (g / C::NSLOT) & 1u, p.timeout_ns);
+        }
+      }
+      __syncthreads();
+      return;
+    }
+    seq += nchunks;
+  }
+}
+
+}  // namespace csd
+
+#endif  // CSD_ENGINE_CUH

@@ -1,0 +1,82 @@
+// Launch parameters and kernel descriptors shared by the host runtime
+// (libcsd.so, compiled by nvcc/g++) and the JIT-compiled stencil kernels
+// (NVRTC).  Plain C layout, no system headers, identical on both sides.
+#ifndef CSD_PARAMS_H
+#define CSD_PARAMS_H
+
+#define CSD_MAX_FIELDS 8
+#define CSD_DESC_MAGIC 0x43534431u /* "CSD1" */
+
+#define CSD_LOADER_TMA 0
+#define CSD_LOADER_LDG 1
+
+#define CSD_BC_NONE 0
+#define CSD_BC_DIRICHLET 1
+#define CSD_BC_NEUMANN 2
+#define CSD_BC_PERIODIC 3
+#define CSD_BC_REFLECTING 4
+
+#define CSD_ERR_TIMEOUT 0x7001
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+// Opaque 128-byte TMA descriptor (same size/alignment as CUtensorMap).
+typedef struct __attribute__((aligned(64))) csd_tmap {
+  unsigned long long opaque[16];
+} csd_tmap;
+
+// Everything a stencil kernel needs at launch.  Arrays are viewed as 3-D
+// (Z, Y, X) with X innermost; a 2-D array (rows, cols) is (rows, 1, cols),
+// a 1-D array (n) is (1, 1, n).  All fields share one shape.
+typedef struct __attribute__((aligned(64))) csd_params {
+  csd_tmap tmap[CSD_MAX_FIELDS];      // TMA descriptors of the inputs
+  const void* in[CSD_MAX_FIELDS];     // input base pointers
+  void* out[CSD_MAX_FIELDS];          // output base pointers
+  long long dims[3];                  // full extents (Z, Y, X), halo included
+  long long pitch_y;                  // elements between consecutive Y
+  long long pitch_z;                  // elements between consecutive Z
+  int halo[3];                        // array halo per internal dim (Z, Y, X)
+  int interior[3];                    // dims - 2 * halo
+  int tiles[3];                       // x tiles, y tiles, z chunks
+  int items;                          // tiles[0] * tiles[1] * tiles[2]
+  int zchunk;                         // output rows of Z per work item
+  int xbase;                          // X origin of tile 0 (halo rounded down to 16 B)
+  int vec_store;                      // 1 when 16-byte output stores are aligned
+  int bc_mode;                        // CSD_BC_* applied to the inputs on load
+  int pad0;
+  double bc_value;                    // Dirichlet value for bc_mode
+  int* err;                           // device error word (0 = ok)
+  unsigned long long timeout_ns;      // bound on every wait
+} csd_params;
+
+// Compile-time configuration of a kernel, exported by each JIT module as
+// `extern "C" __device__ const csd_kernel_desc <name>_desc`.
+typedef struct csd_kernel_desc {
+  unsigned int magic;
+  int ndim;          // stencil dimensionality (1-3)
+  int nin, nout;     // fields read / written
+  int dtype_bytes;   // 4 or 8
+  int rz, ry, rx;    // stencil radius per internal dim (whole temporal chain)
+  int rows;          // Z rows per streaming step
+  int tile_y, tile_x;
+  int vec;           // X points per thread
+  int threads;
+  int stages;        // chunks in flight
+  int nslot;         // ring slots
+  int halo_chunks;
+  int pad_left, box_w, box_h;
+  int smem_bytes;
+  int zchunk;        // default Z rows per work item
+  int temporal;      // stencil steps per pass
+  int bc_mode;       // CSD_BC_* fused into the staging (0 = none)
+  int min_blocks;
+  int align;         // elements per 16 bytes
+} csd_kernel_desc;
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif  // CSD_PARAMS_H

@@ -1,0 +1,448 @@
+"""Dialect 1 -> Dialect 3 lowering (reference: cutile/lowering/stencil_to_target.py).
+
+``_extract_meta`` walks a D1 ``FuncOp`` the way the reference does
+(stencil_to_target.py:163-252): distinct ``(array, offset)`` accesses in
+first-use order with view names such as ``u_m1_0``, input names ``u, v, w``
+(or the parameter names for fused kernels), closure constants and the
+boundary.  The body becomes an exact SSA program (``cutile.lowering.expr``)
+instead of a Python expression string.
+
+``_build_kernel_op`` produces a ``cutile.kernel`` op that carries both the
+reference's properties (kernel_name, tile_shape, halo, ndim, input_names,
+expression(s), grid_order, output_names, constants) and the B200 engine's
+(dtype, radius, accesses, ssa_body, engine tile, temporal depth, layout,
+boundary mode).  The kernel body region keeps the reference's skeleton of
+``bid`` / ``slice`` / ``load`` / ``store`` ops; the host program keeps the
+``launch`` / ``for_loop`` structure.
+"""
+
+from __future__ import annotations
+
+from typing import Sequence
+
+from cutile.dialects.cutile_stencil.dialect import AccessOp, FuncOp
+from cutile.dialects.cutile_target import (
+    BidOp,
+    ForLoopOp,
+    HostProgramOp,
+    KernelOp,
+    LaunchOp,
+    LoadOp,
+    ReturnOp,
+    SliceOp,
+    StoreOp,
+)
+from cutile.ir.core import (
+    ArrayAttr,
+    Block,
+    IndexType,
+    IntAttr,
+    ModuleOp,
+    Region,
+    StringAttr,
+)
+from cutile.lowering.expr import Program, build_program
+
+_IDX = IndexType()
+
+
+class _AccessInfo:
+    """One distinct ``(array_index, offsets)`` access."""
+
+    __slots__ = ("array_index", "offsets", "view_name")
+
+    def __init__(self, array_index: int, offsets: tuple[int, ...], view_name: str):
+        self.array_index = array_index
+        self.offsets = offsets
+        self.view_name = view_name
+
+    def __repr__(self):
+        return f"_AccessInfo({self.array_index}, {self.offsets}, {self.view_name!r})"
+
+
+class _StencilMeta:
+    """Metadata of one kernel (single stencil or fused group)."""
+
+    def __init__(self) -> None:
+        self.name = ""
+        self.ndim = 2
+        self.order = 2
+        self.dtype = "float64"
+        self.num_inputs = 1
+        self.input_names: list[str] = []
+        self.accesses: list[_AccessInfo] = []
+        self.expression = ""
+        self.constants: dict[str, float] = {}
+        self.boundary: dict | None = None
+        self.kernel_constants: list[float] = []
+        self.expressions: list[str] = []
+        self.output_names: list[str] = []
+        self.stencil_inputs: list[list[str]] = []
+        self.programs: list[Program] = []
+
+    @property
+    def num_outputs(self) -> int:
+        return max(1, len(self.expressions))
+
+    def output_views(self) -> list[str]:
+        if self.num_outputs == 1:
+            return ["out"]
+        return [f"out_{k}" for k in range(self.num_outputs)]
+
+    def output_params(self) -> list[str]:
+        if self.output_names:
+            return [f"{n}_out" for n in self.output_names]
+        return ["u_out"]
+
+    def halo(self) -> tuple[int, ...]:
+        """Stencil footprint per dimension (max |offset|)."""
+        h = [0] * self.ndim
+        for a in self.accesses:
+            for d, o in enumerate(a.offsets):
+                h[d] = max(h[d], abs(o))
+        return tuple(h)
+
+
+def _default_input_names(n: int) -> list[str]:
+    defaults = list("uvwxyz")
+    return [defaults[i] if i < len(defaults) else f"arr{i}" for i in range(n)]
+
+
+def _format_offset(off: int) -> str:
+    if off == 0:
+        return "0"
+    return f"p{off}" if off > 0 else f"m{abs(off)}"
+
+
+def _offset_expr(halo_var: str, off: int, *, add_n: bool = False, n_var: str = "n") -> str:
+    base = halo_var if off == 0 else (f"{halo_var} + {off}" if off > 0 else f"{halo_var} - {abs(off)}")
+    return f"{base} + {n_var}" if add_n else base
+
+
+def grid_order(ndim: int) -> tuple[int, ...]:
+    """Array dims in block-index order (stencil_to_target.py:475-488): ``(0,)``,
+    ``(0, 1)``, ``(1, 0, 2)``.  The B200 engine instead streams dim 0 inside each
+    block and spreads work items over the grid X-fastest; the attribute is kept
+    for the reference's D3 consumers."""
+    if ndim <= 2:
+        return tuple(range(ndim))
+    return tuple(range(ndim - 2, -1, -1)) + (ndim - 1,)
+
+
+def fit_tiles(tiles, shape, halos) -> tuple[int, ...]:
+    """Clamp each tile dim to the next power of two >= the interior
+    (the reference's ``_fit_tiles``, target_to_python.py:305-321)."""
+    fitted = []
+    for t, n, h in zip(tiles, shape, halos):
+        interior = max(1, n - 2 * h)
+        fitted.append(min(t, 1 << max(0, (interior - 1).bit_length())))
+    return tuple(fitted)
+
+
+def _func_and_block(module: ModuleOp):
+    for op in module.body.block.ops:
+        if isinstance(op, FuncOp):
+            return op, op.body.blocks[0]
+    raise ValueError("No cutile_stencil.FuncOp found in module")
+
+
+def _arg_names(func_op: FuncOp, block: Block) -> list[str]:
+    if func_op.arg_names is not None:
+        return [a.data for a in func_op.arg_names.data]
+    return _default_input_names(len(block.args))
+
+
+def _access_keys(block: Block, names: Sequence[str]) -> set:
+    keys = set()
+    for op in block.ops:
+        if isinstance(op, AccessOp):
+            idx = next((i for i, a in enumerate(block.args) if op.field is a), 0)
+            keys.add((names[idx], tuple(op.offset.offsets)))
+    return keys
+
+
+def _field_dtype(meta_dtype: str) -> str:
+    return "f32" if meta_dtype in ("float32", "fp32") else "f64"
+
+
+def _extract_meta(func_op: FuncOp, block: Block, spatial_term_order: bool | None = None, *,
+                  input_names: Sequence[str] | None = None,
+                  kernel_constants: list[float] | None = None,
+                  shared_accesses: list | None = None,
+                  dtype: str | None = None) -> _StencilMeta:
+    """Metadata of one stencil (stencil_to_target.py:163-252).
+
+    ``shared_accesses`` (a list of ``_AccessInfo``) makes several stencils
+    index one merged access list (fused kernels); ``dtype`` overrides the
+    declared dtype (kernels are specialised for the arrays' actual dtype).
+    """
+    meta = _StencilMeta()
+    meta.name = func_op.func_name.data
+    meta.ndim = func_op.ndim.data
+    meta.order = func_op.order.data
+    if func_op.dtype is not None:
+        meta.dtype = func_op.dtype.data
+    if dtype is not None:
+        meta.dtype = dtype
+    meta.num_inputs = len(block.args)
+    if input_names is not None:
+        if len(input_names) != meta.num_inputs:
+            raise ValueError(f"{meta.name}: {len(input_names)} input names for "
+                             f"{meta.num_inputs} arrays")
+        meta.input_names = list(input_names)
+    else:
+        meta.input_names = _default_input_names(meta.num_inputs)
+    if kernel_constants is not None:
+        meta.kernel_constants = kernel_constants
+    if func_op.constants is not None:
+        for key, val in func_op.constants.data.items():
+            meta.constants[key] = val.data
+    if func_op.boundary is not None:
+        meta.boundary = {"type": func_op.boundary.bc_type_str}
+        if func_op.boundary.has_value:
+            meta.boundary["value"] = func_op.boundary.value.data
+
+    accesses = shared_accesses if shared_accesses is not None else []
+    by_view = {a.view_name: k for k, a in enumerate(accesses)}
+    own: list[_AccessInfo] = []
+    access_index = {}
+    access_offsets = {}
+    for op in block.ops:
+        if isinstance(op, AccessOp):
+            offsets = tuple(op.offset.offsets)
+            arr_idx = next((i for i, a in enumerate(block.args) if op.field is a), 0)
+            view = f"{meta.input_names[arr_idx]}_" + "_".join(_format_offset(o) for o in offsets)
+            if view not in by_view:
+                by_view[view] = len(accesses)
+                accesses.append(_AccessInfo(arr_idx, offsets, view))
+            if all(a.view_name != view for a in own):
+                own.append(accesses[by_view[view]])
+            access_index[op.res] = by_view[view]
+            access_offsets[op.res] = offsets
+    meta.accesses = own if shared_accesses is not None else accesses
+    if spatial_term_order is None:
+        spatial_term_order = False
+    prog = build_program(block, access_index, _field_dtype(meta.dtype),
+                         spatial_order=bool(spatial_term_order), access_offsets=access_offsets)
+    meta.programs = [prog]
+    meta.expression = prog.expression
+    meta.expressions = [meta.expression]
+    return meta
+
+
+def fused_name(names: Sequence[str]) -> str:
+    return "_".join(names) if len(names) <= 3 else f"{names[0]}_and_{len(names) - 1}_others"
+
+
+def extract_fused_meta(modules: Sequence[ModuleOp], spatial_term_order: bool | None = None,
+                       dtype: str | None = None) -> _StencilMeta:
+    """Merge several stencils into one multi-output kernel's metadata
+    (stencil_to_target.py:968-1031): inputs are matched by parameter name,
+    each distinct ``(field, offset)`` is one access shared by every output."""
+    if not modules:
+        raise ValueError("At least one module is required for fusion")
+    funcs = [_func_and_block(m) for m in modules]
+    stencil_inputs = [_arg_names(f, b) for f, b in funcs]
+    inputs: list[str] = []
+    for names in stencil_inputs:
+        for n in names:
+            if n not in inputs:
+                inputs.append(n)
+    shared: list[_AccessInfo] = []
+    metas = [
+        _extract_meta(f, b, spatial_term_order, input_names=names, shared_accesses=shared,
+                      dtype=dtype)
+        for (f, b), names in zip(funcs, stencil_inputs)
+    ]
+    names = [m.name for m in metas]
+    if len(set(names)) != len(names):
+        raise ValueError(f"fused stencils must have distinct names, got {names}")
+    for m in metas[1:]:
+        if m.ndim != metas[0].ndim:
+            raise ValueError(f"cannot fuse {m.ndim}D {m.name} with {metas[0].ndim}D {metas[0].name}")
+        if m.dtype != metas[0].dtype:
+            raise ValueError(f"cannot fuse {m.dtype} {m.name} with {metas[0].dtype} {metas[0].name}")
+    fused = _StencilMeta()
+    fused.name = fused_name(names)
+    fused.ndim = metas[0].ndim
+    fused.order = max(m.order for m in metas)
+    fused.dtype = metas[0].dtype
+    fused.num_inputs = len(inputs)
+    fused.input_names = inputs
+    # re-index accesses against the merged input list
+    for a, m in _owners(shared, metas):
+        a.array_index = inputs.index(m.input_names[a.array_index])
+    fused.accesses = shared
+    fused.expressions = [m.expression for m in metas]
+    fused.expression = fused.expressions[0]
+    fused.output_names = names
+    fused.stencil_inputs = stencil_inputs
+    fused.programs = [m.programs[0] for m in metas]
+    for m in metas:
+        fused.constants.update(m.constants)
+    return fused
+
+
+def _owners(shared, metas):
+    done = set()
+    for m in metas:
+        for a in m.accesses:
+            if id(a) not in done:
+                done.add(id(a))
+                yield a, m
+
+
+# --------------------------------------------------------------------------- #
+# Target IR builders
+# --------------------------------------------------------------------------- #
+
+
+def _build_kernel_body(meta: _StencilMeta) -> Region:
+    ndim = meta.ndim
+    halo_vars = ["HX", "HY", "HZ"][:ndim]
+    n_vars = ["nx", "ny", "nz"][:ndim]
+    block = Block(arg_types=[_IDX] * (meta.num_inputs + meta.num_outputs))
+    for d in range(ndim):
+        block.add_op(BidOp.build(properties={"axis": IntAttr(d)}, result_types=[_IDX]))
+    for info in meta.accesses:
+        prev = block.args[info.array_index]
+        for d in range(ndim):
+            props = {"axis": IntAttr(d),
+                     "start": StringAttr(_offset_expr(halo_vars[d], info.offsets[d])),
+                     "stop": StringAttr(_offset_expr(halo_vars[d], info.offsets[d], add_n=True,
+                                                     n_var=n_vars[d]))}
+            if d == ndim - 1:
+                props["var_name"] = StringAttr(info.view_name)
+            s = SliceOp.build(properties=props, operands=[prev], result_types=[_IDX])
+            block.add_op(s)
+            prev = s.result
+        block.add_op(LoadOp.build(properties={"view_name": StringAttr(info.view_name)},
+                                  operands=[prev], result_types=[_IDX]))
+    for k, view in enumerate(meta.output_views()):
+        prev = block.args[meta.num_inputs + k]
+        for d in range(ndim):
+            props = {"axis": IntAttr(d), "start": StringAttr(halo_vars[d]),
+                     "stop": StringAttr(f"{halo_vars[d]} + {n_vars[d]}")}
+            if d == ndim - 1:
+                props["var_name"] = StringAttr(view)
+            s = SliceOp.build(properties=props, operands=[prev], result_types=[_IDX])
+            block.add_op(s)
+            prev = s.result
+        block.add_op(StoreOp.build(operands=[prev, prev]))
+    block.add_op(ReturnOp.build())
+    return Region([block])
+
+
+def _build_kernel_op(meta: _StencilMeta, tile_sizes: tuple[int, ...], halo_widths: tuple[int, ...],
+                     kernel_hints: dict | None = None, *, temporal_steps: int = 1,
+                     layout: str = "flat", brick_size: int = 0, boundary_mode: str = "none"
+                     ) -> KernelOp:
+    props: dict = {
+        "kernel_name": StringAttr(meta.name),
+        "tile_shape": ArrayAttr([IntAttr(t) for t in tile_sizes]),
+        "halo": ArrayAttr([IntAttr(h) for h in halo_widths]),
+        "ndim": IntAttr(meta.ndim),
+        "input_names": ArrayAttr([StringAttr(n) for n in meta.input_names]),
+        "expression": StringAttr(meta.expression),
+        "grid_order": ArrayAttr([IntAttr(d) for d in grid_order(meta.ndim)]),
+        "dtype": StringAttr(meta.dtype),
+        "radius": ArrayAttr([IntAttr(r) for r in meta.halo()]),
+        "accesses": ArrayAttr([
+            ArrayAttr([IntAttr(a.array_index)] + [IntAttr(o) for o in a.offsets])
+            for a in meta.accesses]),
+        "ssa_body": ArrayAttr([
+            ArrayAttr([StringAttr(line) for line in p.lines] + [StringAttr(f"return {p.result}")])
+            for p in meta.programs]),
+        "temporal_steps": IntAttr(temporal_steps),
+        "layout": StringAttr(layout),
+        "brick_size": IntAttr(brick_size),
+        "boundary_mode": StringAttr(boundary_mode),
+    }
+    if meta.num_outputs > 1:
+        props["expressions"] = ArrayAttr([StringAttr(x) for x in meta.expressions])
+        props["output_names"] = ArrayAttr([StringAttr(n) for n in meta.output_names])
+    if kernel_hints:
+        items: list = []
+        for key in sorted(kernel_hints):
+            items.append(StringAttr(str(key)))
+            items.append(StringAttr(repr(kernel_hints[key])))
+        props["kernel_hints"] = ArrayAttr(items)
+    if meta.constants:
+        items = []
+        for k, v in sorted(meta.constants.items()):
+            items.append(StringAttr(k))
+            items.append(StringAttr(repr(v)))
+        props["constants"] = ArrayAttr(items)
+    return KernelOp.build(properties=props, regions=[_build_kernel_body(meta)])
+
+
+def _launch_signature(meta: _StencilMeta) -> str:
+    outs = ", ".join(meta.output_params())
+    if meta.num_inputs > 1 or meta.output_names:
+        return f"launch_{meta.name}({', '.join(meta.input_names)}, {outs}, stream=None)"
+    return f"launch_{meta.name}(u_in, {outs}, stream=None)"
+
+
+def _build_host(meta: _StencilMeta, temporal_steps: int) -> HostProgramOp:
+    """Host launcher skeleton: one engine launch (temporal chains run inside it).
+
+    The reference's temporal host is a ``for_loop`` of ``T`` launches
+    (stencil_to_target.py:783-843); here the loop count is recorded on the
+    ``for_loop`` op with a single launch in its body, and the engine realises
+    the ``T`` steps in one pass.
+    """
+    args = ", ".join(meta.input_names) if (meta.num_inputs > 1 or meta.output_names) else "u_in"
+    launch = LaunchOp.build(properties={
+        "kernel_name": StringAttr(f"{meta.name}_kernel"),
+        "grid_expr": StringAttr("persistent"),
+        "args_expr": StringAttr(f"({args}, {', '.join(meta.output_params())})"),
+    })
+    if temporal_steps > 1:
+        body_op = ForLoopOp.build(properties={"count": IntAttr(temporal_steps)},
+                                  regions=[Region([Block([launch])])])
+    else:
+        body_op = launch
+    return HostProgramOp.build(properties={
+        "program_name": StringAttr(_launch_signature(meta)),
+        "preamble": StringAttr("stream = current stream if None"),
+    }, regions=[Region([Block([body_op])])])
+
+
+def lower_to_target_ir(module: ModuleOp, tile_sizes: tuple[int, ...], halo_widths: tuple[int, ...],
+                       temporal_steps: int = 1, boundary_spec: dict | None = None,
+                       kernel_hints: dict | None = None, spatial_term_order: bool | None = None,
+                       *, dtype: str | None = None, layout: str = "flat", brick_size: int = 0,
+                       boundary_mode: str = "none") -> ModuleOp:
+    """Dialect 1 module -> Dialect 3 module (``cutile.kernel`` + host program)."""
+    func_op, block = _func_and_block(module)
+    meta = _extract_meta(func_op, block, spatial_term_order, dtype=dtype)
+    if boundary_spec is None and meta.boundary is not None:
+        boundary_spec = meta.boundary
+    kernel = _build_kernel_op(meta, tile_sizes, halo_widths, kernel_hints,
+                              temporal_steps=temporal_steps, layout=layout,
+                              brick_size=brick_size, boundary_mode=boundary_mode)
+    host = _build_host(meta, temporal_steps)
+    target = ModuleOp([kernel, host])
+    if boundary_spec is not None:
+        items = [StringAttr(boundary_spec.get("type", "dirichlet"))]
+        if "value" in boundary_spec:
+            items.append(StringAttr(str(boundary_spec["value"])))
+        target.attributes["boundary"] = ArrayAttr(items)
+        target.attributes["stencil_name"] = StringAttr(meta.name)
+        target.attributes["stencil_ndim"] = IntAttr(meta.ndim)
+        target.attributes["stencil_halo"] = ArrayAttr([IntAttr(h) for h in halo_widths])
+    return target
+
+
+def lower_fused_to_target_ir(modules: Sequence[ModuleOp], tile_sizes: tuple[int, ...],
+                             halo_widths: tuple[int, ...], kernel_hints: dict | None = None,
+                             spatial_term_order: bool | None = None, *, dtype: str | None = None,
+                             boundary_mode: str = "none") -> ModuleOp:
+    meta = extract_fused_meta(modules, spatial_term_order, dtype=dtype)
+    kernel = _build_kernel_op(meta, tile_sizes, halo_widths, kernel_hints,
+                              boundary_mode=boundary_mode)
+    return ModuleOp([kernel, _build_host(meta, 1)])
+
+
+__all__ = ["lower_to_target_ir", "lower_fused_to_target_ir", "extract_fused_meta", "fused_name",
+           "grid_order", "fit_tiles", "_extract_meta", "_StencilMeta", "_AccessInfo"]

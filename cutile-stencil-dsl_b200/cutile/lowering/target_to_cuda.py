@@ -1,0 +1,284 @@
+"""Dialect 3 -> CUDA C++ for the sm_100a stencil engine.
+
+Replaces the reference's Dialect 3 -> cuTile Python emitter
+(cutile/lowering/target_to_python.py:464-526).  For each ``cutile.kernel``:
+
+* the body becomes a device functor ``Body_<name>::compute``: for every
+  distinct ``(field, z offset, y offset)`` it loads one row *strip* from the
+  staged tile (16-byte shared-memory vector loads), then evaluates each of
+  the thread's ``VEC`` points with one statement per SSA op of the DSL body,
+  in DSL order, using round-to-nearest intrinsics (``__dadd_rn`` ...) so no
+  multiply-add contraction or re-association can change a bit;
+* two kernels instantiate the engine template around it: ``<name>_tma``
+  (TMA tile copies) and ``<name>_ldg`` (cp.async copies, for arrays whose
+  row pitch is not 16-byte aligned);
+* ``<name>_desc`` exports the compile-time configuration to the host runtime.
+
+Constants are emitted as exact hexadecimal float literals (the reference
+needed a device array of float64 constants because cuTile rounds Python
+scalars to float32, target_to_python.py:170-180, 429-451).
+"""
+
+from __future__ import annotations
+
+import math
+import struct
+
+from cutile.dialects.cutile_target import KernelOp
+from cutile.ir.core import ModuleOp
+
+BC_CODES = {"none": "CSD_BC_NONE", "dirichlet": "CSD_BC_DIRICHLET", "neumann": "CSD_BC_NEUMANN",
+            "periodic": "CSD_BC_PERIODIC", "reflecting": "CSD_BC_REFLECTING"}
+
+_CTYPE = {"f32": "float", "f64": "double", "w": "double", "b": "bool", "wb": "bool"}
+
+
+def hex_literal(value: float, ctype: str = "double") -> str:
+    """Exact C literal for *value* in *ctype* (``float`` literals are the
+    float32 rounding of the double, as NumPy rounds a Python float)."""
+    if ctype == "float":
+        v32 = struct.unpack("<f", struct.pack("<f", value))[0]
+        if math.isfinite(v32):
+            return f"{float(v32).hex()}f"
+        bits = struct.unpack("<I", struct.pack("<f", v32))[0]
+        return f"__int_as_float(0x{bits:08x})"
+    if math.isfinite(value):
+        return float(value).hex()
+    bits = struct.unpack("<Q", struct.pack("<d", value))[0]
+    return f"__longlong_as_double(0x{bits:016x}LL)"
+
+
+def _internal_offsets(ndim: int, offsets) -> tuple[int, int, int]:
+    if ndim == 3:
+        return tuple(offsets)
+    if ndim == 2:
+        return (offsets[0], 0, offsets[1])
+    return (0, 0, offsets[0])
+
+
+def _parse_line(line: str):
+    """``v3 = addf v1, a0 : f64`` -> ("v3", "addf", ["v1", "a0"], "f64", extra)."""
+    if line.startswith("return "):
+        return ("", "return", [line.split()[1]], "", None)
+    lhs, rhs = line.split(" = ", 1)
+    body, typ = rhs.rsplit(" : ", 1)
+    parts = body.split(" ", 1)
+    op = parts[0]
+    rest = parts[1] if len(parts) > 1 else ""
+    extra = None
+    if op == "const":
+        return (lhs, op, [], typ, float(rest))
+    if "@" in rest:
+        rest, extra = rest.split(" @")
+    args = [a.strip() for a in rest.split(",")] if rest else []
+    return (lhs, op, args, typ, extra)
+
+
+class _BodyEmitter:
+    def __init__(self, prefix: str):
+        self.prefix = prefix
+        self.types: dict[str, str] = {}
+        self.consts: dict[str, float] = {}
+        self.lines: list[str] = []
+
+    def name(self, v: str) -> str:
+        return v if v.startswith("a") else f"{self.prefix}{v}"
+
+    def conv(self, v: str, to: str) -> str:
+        """Operand *v* as C type of numpy kind *to* (f32/f64)."""
+        t = self.types[v]
+        if t == "w" and v in self.consts:
+            return hex_literal(self.consts[v], "float" if to == "f32" else "double")
+        n = self.name(v)
+        if t in ("w", "f64") and to == "f32":
+            return f"(float){n}"
+        if t == "f32" and to == "f64":
+            return f"(double){n}"
+        return n
+
+    def emit(self, lines: list[str], access_types: dict[str, str]) -> str:
+        self.types.update(access_types)
+        result = None
+        for raw in lines:
+            lhs, op, args, typ, extra = _parse_line(raw)
+            if op == "return":
+                result = args[0]
+                continue
+            self.types[lhs] = typ
+            if op == "const":
+                self.consts[lhs] = extra
+                continue
+            ct = _CTYPE[typ]
+            tgt = "f64" if typ in ("w", "f64") else typ
+            sfx = "f" if tgt == "f32" else "d"
+            if op in ("addf", "subf", "mulf", "divf"):
+                fn = {"addf": "add", "subf": "sub", "mulf": "mul", "divf": "div"}[op]
+                expr = f"__{sfx}{fn}_rn({self.conv(args[0], tgt)}, {self.conv(args[1], tgt)})"
+            elif op == "negf":
+                expr = f"-({self.conv(args[0], tgt)})"
+            elif op == "absf":
+                expr = f"{'fabsf' if tgt == 'f32' else 'fabs'}({self.conv(args[0], tgt)})"
+            elif op == "sqrt":
+                expr = f"__{sfx}sqrt_rn({self.conv(args[0], tgt)})"
+            elif op in ("maxf", "minf"):
+                fn = "csd_max" if op == "maxf" else "csd_min"
+                expr = f"{fn}({self.conv(args[0], tgt)}, {self.conv(args[1], tgt)})"
+            elif op.startswith("cmp."):
+                pred = op.split(".", 1)[1]
+                sym = {"oeq": "==", "ogt": ">", "oge": ">=", "olt": "<", "ole": "<=",
+                       "one": "!=", "une": "!="}[pred]
+                cmp_t = extra or "f64"
+                a, b = self.conv(args[0], cmp_t), self.conv(args[1], cmp_t)
+                if pred == "one":  # ordered not-equal: false on NaN
+                    expr = f"(({a}) < ({b}) || ({a}) > ({b}))"
+                else:
+                    expr = f"(({a}) {sym} ({b}))"
+            elif op == "select":
+                c = self.name(args[0]) if self.types[args[0]] in ("b", "wb") else self.conv(args[0], "f64")
+                expr = f"({c} ? {self.conv(args[1], tgt)} : {self.conv(args[2], tgt)})"
+            else:
+                raise ValueError(f"unknown SSA op {op!r}")
+            self.lines.append(f"const {ct} {self.name(lhs)} = {expr};")
+        return result
+
+    def result_as(self, v: str, store_t: str) -> str:
+        t = self.types[v]
+        if t in ("b", "wb"):
+            return f"({store_t})({self.name(v)} ? 1 : 0)"
+        if t == "w" and v in self.consts:
+            return hex_literal(self.consts[v], store_t)
+        return f"({store_t}){self.name(v)}"
+
+
+def emit_body(kernel: KernelOp) -> str:
+    """Device functor for the kernel's stencil body(ies)."""
+    name = kernel.kernel_name.data
+    ndim = kernel.ndim.data
+    dtype = kernel.dtype.data
+    field_t = "f32" if dtype in ("float32", "fp32") else "f64"
+    store_t = "float" if field_t == "f32" else "double"
+    accesses = [tuple(a.data for a in acc) for acc in kernel.accesses.data]
+    # group accesses by (field, dz, dy) -> x range
+    groups: dict[tuple, list] = {}
+    acc_info = []
+    for j, (f, *offs) in enumerate(accesses):
+        dz, dy, dx = _internal_offsets(ndim, offs)
+        key = (f, dz, dy)
+        groups.setdefault(key, []).append(dx)
+        acc_info.append((key, dx))
+    gkeys = list(groups)
+    out = [f"struct Body_{name} {{",
+           "  template <class C>",
+           "  __device__ __forceinline__ static void compute(const csd::TileView<C>& t, int r, int y,",
+           "                                                 int x, csd::OutPack<typename C::T, "
+           "C::NOUT, C::VEC>& o) {"]
+    for gi, key in enumerate(gkeys):
+        f, dz, dy = key
+        lo, hi = min(groups[key]), max(groups[key])
+        out.append(f"    const auto s{gi} = t.template strip<{f}, {dz}, {dy}, {lo}, {hi}>(r, y, x);")
+    out.append("#pragma unroll")
+    out.append("    for (int k = 0; k < C::VEC; ++k) {")
+    access_types = {}
+    for j, (key, dx) in enumerate(acc_info):
+        gi = gkeys.index(key)
+        lo = min(groups[key])
+        out.append(f"      const {store_t} a{j} = s{gi}.v[k + {dx - lo}];")
+        access_types[f"a{j}"] = field_t
+    for m, prog in enumerate(kernel.ssa_body.data):
+        em = _BodyEmitter(f"p{m}_")
+        res = em.emit([s.data for s in prog], access_types)
+        for line in em.lines:
+            out.append("      " + line)
+        out.append(f"      o.v[{m}][k] = {em.result_as(res, store_t)};")
+    out.append("    }")
+    out.append("  }")
+    out.append("};")
+    return "\n".join(out)
+
+
+def _internal_radius(ndim: int, radius) -> tuple[int, int, int]:
+    r = list(radius)
+    if ndim == 3:
+        return (r[0], r[1], r[2])
+    if ndim == 2:
+        return (r[0], 0, r[1])
+    return (0, 0, r[0])
+
+
+def engine_params(kernel: KernelOp) -> dict:
+    """Template parameters of the engine instance described by *kernel*."""
+    ndim = kernel.ndim.data
+    dtype = kernel.dtype.data
+    tile = [a.data for a in kernel.tile_shape.data]
+    hints = {}
+    if kernel.kernel_hints is not None:
+        items = [a.data for a in kernel.kernel_hints.data]
+        hints = {k: eval(v, {}) for k, v in zip(items[0::2], items[1::2])}  # repr'd ints
+    if ndim == 3:
+        rows, ty, tx = tile
+    elif ndim == 2:
+        rows, tx = tile
+        ty = 1
+    else:
+        (tx,) = tile
+        rows, ty = 1, 1
+    rz, ry, rx = _internal_radius(ndim, [a.data for a in kernel.radius.data])
+    nout = len(kernel.ssa_body.data)
+    nin = len(kernel.input_names.data)
+    return {
+        "T": "float" if dtype in ("float32", "fp32") else "double",
+        "dtype_bytes": 4 if dtype in ("float32", "fp32") else 8,
+        "NIN": nin, "NOUT": nout, "RZ": rz, "RY": ry, "RX": rx, "ROWS": rows, "TY": ty, "TX": tx,
+        "NT": int(hints.get("threads", 256)), "STAGES": int(hints.get("stages", 1)),
+        "TEMPORAL": kernel.temporal_steps.data if kernel.temporal_steps is not None else 1,
+        "BC": BC_CODES[kernel.boundary_mode.data if kernel.boundary_mode is not None else "none"],
+        "MINB": int(hints.get("min_blocks", 1)), "ZCHUNK": int(hints.get("zchunk", 64)),
+        "ndim": ndim,
+    }
+
+
+def emit_cuda(module: ModuleOp, preamble: bool = True) -> str:
+    """CUDA translation unit for the kernel(s) in a D3 module (``preamble=False``
+    gives just the kernels, to append to another unit)."""
+    kernels = [op for op in module.body.block.ops if isinstance(op, KernelOp)]
+    if not kernels:
+        raise ValueError("No KernelOp found in target IR module")
+    parts = ["// Generated B200 stencil kernel(s). Do not edit.",
+             '#include "csd/engine.cuh"', "",
+             "__device__ __forceinline__ double csd_max(double a, double b) "
+             "{ return (a != a || a > b) ? a : b; }",
+             "__device__ __forceinline__ double csd_min(double a, double b) "
+             "{ return (a != a || a < b) ? a : b; }",
+             "__device__ __forceinline__ float csd_max(float a, float b) "
+             "{ return (a != a || a > b) ? a : b; }",
+             "__device__ __forceinline__ float csd_min(float a, float b) "
+             "{ return (a != a || a < b) ? a : b; }", ""]
+    if not preamble:
+        parts = []
+    for kernel in kernels:
+        name = kernel.kernel_name.data
+        p = engine_params(kernel)
+        parts.append(f"// expression: {kernel.expression.data}")
+        parts.append(emit_body(kernel))
+        parts.append("")
+        for suffix, loader in (("tma", "CSD_LOADER_TMA"), ("ldg", "CSD_LOADER_LDG")):
+            cfg = (f"csd::Cfg<{p['T']}, {p['NIN']}, {p['NOUT']}, {p['RZ']}, {p['RY']}, {p['RX']}, "
+                   f"{p['ROWS']}, {p['TY']}, {p['TX']}, {p['NT']}, {p['STAGES']}, {p['TEMPORAL']}, "
+                   f"{loader}, {p['BC']}>")
+            parts.append(f"typedef {cfg} Cfg_{name}_{suffix};")
+            parts.append(f'extern "C" __global__ void __launch_bounds__({p["NT"]}, {p["MINB"]})')
+            parts.append(f"{name}_{suffix}(const __grid_constant__ csd_params p) {{")
+            parts.append(f"  csd::stream_engine<Cfg_{name}_{suffix}, Body_{name}>(p);")
+            parts.append("}")
+        c = f"Cfg_{name}_tma"
+        parts.append(f'extern "C" __device__ const csd_kernel_desc {name}_desc = {{')
+        parts.append(f"  CSD_DESC_MAGIC, {p['ndim']}, {c}::NIN, {c}::NOUT, (int)sizeof({c}::T),")
+        parts.append(f"  {c}::RZ * {c}::TEMPORAL, {c}::RY * {c}::TEMPORAL, {c}::RX * {c}::TEMPORAL,")
+        parts.append(f"  {c}::ROWS, {c}::TY, {c}::TX, {c}::VEC, {c}::NT, {c}::STAGES, {c}::NSLOT,")
+        parts.append(f"  {c}::HC * {c}::TEMPORAL, {c}::PADL, {c}::BOXW, {c}::BOXH, {c}::SMEM_BYTES,")
+        parts.append(f"  {p['ZCHUNK']}, {c}::TEMPORAL, {c}::BC, {p['MINB']}, {c}::ALIGN}};")
+        parts.append("")
+    return "\n".join(parts) + "\n"
+
+
+__all__ = ["emit_cuda", "emit_body", "engine_params", "hex_literal"]

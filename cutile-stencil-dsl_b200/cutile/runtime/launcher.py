@@ -1,0 +1,525 @@
+"""``compile`` / ``compile_fused`` / ``CompileResult`` -- the drop-in boundary.
+
+Mirrors cutile/runtime/launcher.py of the reference (lines 27-728): same
+signatures, same ``CompileResult`` fields and methods, same halo / temporal
+semantics.  What the result's ``code`` holds differs: instead of cuTile
+Python it is a Python module whose ``launch_<name>`` (and
+``apply_boundary_<name>``, ``step_<name>``, bricked helpers) call the B200
+engine kernels compiled from ``cuda_source`` through libcsd.
+
+Semantics kept from the reference:
+
+* ``temporal_steps`` comes from the reference's pass pipeline (49152-byte
+  budget by default), so ``launch_<name>`` advances the same number of steps
+  per call; intermediate steps see zero halos; the input is not modified;
+* ``align_halo`` pads the innermost halo to 128 bytes (launcher.py:257-273);
+* launch arguments: ``(u_in, u_out)`` for one input, ``(u, v, ..., u_out)``
+  for several (input names ``u v w x y z``), fused kernels take the merged
+  parameter names then ``<member>_out`` each; only output interiors are
+  written.
+
+Extensions: ``temporal_steps=`` forces a depth, ``tile_sizes=`` /
+``kernel_hints=`` override the engine plan, ``dtype=`` overrides the
+declared dtype.  ``num_gpus > 1`` raises: multi-GPU decomposition is not
+part of this backend.
+"""
+
+from __future__ import annotations
+
+import importlib.util
+import json
+import math
+import tempfile
+from dataclasses import dataclass, field, replace
+from typing import Any, Optional
+
+from cutile.dialects.stencil import ApplyOp
+from cutile.runtime.pipeline import Pipeline
+
+
+@dataclass
+class CompileResult:
+    """Result of compiling a stencil (launcher.py:27-231)."""
+
+    name: str
+    code: str
+    ndim: int
+    halo_widths: tuple[int, ...]
+    tile_sizes: tuple[int, ...]
+    temporal_steps: int
+    analysis: dict = field(default_factory=dict)
+    stencil_halo: tuple[int, ...] = field(default=())
+    kernel_hints: dict = field(default_factory=dict)
+    resources: Any = field(default=None)
+    inputs: tuple = ()
+    outputs: tuple = ()
+    cuda_source: str = ""
+    dtype: str = "float64"
+    boundary: Optional[dict] = None
+    layout: str = "flat"
+    brick_size: int = 0
+    _ref_fn: Any = field(default=None, repr=False)
+    _ref_fns: Any = field(default=None, repr=False)
+    _ref_inputs: Any = field(default=None, repr=False)
+    _module: Any = field(default=None, repr=False)
+
+    def emit_to_file(self, path: str) -> None:
+        """Write the generated launcher module to *path* (its CUDA source is
+        embedded; ``emit_cuda_to_file`` writes the ``.cu`` alone)."""
+        with open(path, "w") as f:
+            f.write(self.code)
+
+    def emit_cuda_to_file(self, path: str) -> None:
+        with open(path, "w") as f:
+            f.write(self.cuda_source)
+
+    def load_module(self):
+        """Load the generated launcher module (cached per result)."""
+        if self._module is not None:
+            return self._module
+        with tempfile.NamedTemporaryFile(suffix=".py", delete=False, mode="w") as f:
+            f.write(self.code)
+            tmp_path = f.name
+        spec = importlib.util.spec_from_file_location(f"_gen_{self.name}", tmp_path)
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        self._module = mod
+        return mod
+
+    # -- self checks ---------------------------------------------------------
+    def _np_dtype(self):
+        import numpy as np
+
+        return np.float32 if self.dtype in ("float32", "fp32") else np.float64
+
+    def validate(self, u_input=None, atol: float = 1e-10) -> bool:
+        """Run the kernel once and compare with the stencil function evaluated
+        by NumPy on the same data (launcher.py:76-132): ``temporal_steps``
+        applications, compared on the interior shrunk by ``T * halo`` (the
+        kernel's intermediate steps see zero halos, NumPy's keep the input's)."""
+        import numpy as np
+        import torch
+
+        if self._ref_fns and (len(self._ref_fns) > 1 or len(self.inputs) > 1):
+            return self._validate_multi(atol)
+        if self._ref_fn is None:
+            raise RuntimeError("No reference function available")
+        hw, ndim, T = self.halo_widths, self.ndim, self.temporal_steps
+        if u_input is None:
+            base = 128 if ndim == 1 else 64
+            u_np = np.random.rand(*tuple(base + 2 * T * h for h in hw)).astype(self._np_dtype())
+        else:
+            u_np = np.asarray(u_input, dtype=self._np_dtype())
+        ref = u_np.copy()
+        for _ in range(T):
+            ref = _numpy_apply(ref, self._ref_fn, ndim, hw)
+        launcher = getattr(self.load_module(), f"launch_{self.name}")
+        u_gpu = torch.from_numpy(u_np).cuda()
+        out = torch.zeros_like(u_gpu)
+        launcher(u_gpu, out)
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        inner = tuple(slice(T * h, s - T * h) for h, s in zip(hw, u_np.shape))
+        max_diff = float(np.max(np.abs(ref[inner] - got[inner])))
+        ok = bool(np.allclose(ref[inner], got[inner], atol=atol))
+        print(f"Validation: max_diff={max_diff:.2e}, pass={ok}")
+        return ok
+
+    def _validate_multi(self, atol: float) -> bool:
+        import inspect
+
+        import numpy as np
+        import torch
+
+        from cutile.frontend.elementwise import array_aware
+
+        hw = self.halo_widths
+        base = 128 if self.ndim == 1 else 64
+        shape = tuple(base + 2 * h for h in hw)
+        dt = self._np_dtype()
+        inputs = {n: (np.random.rand(*shape) + 0.5).astype(dt) for n in self.inputs}
+        launcher = getattr(self.load_module(), f"launch_{self.name}")
+        gin = [torch.from_numpy(inputs[n]).cuda() for n in self.inputs]
+        gout = [torch.zeros(shape, dtype=gin[0].dtype, device="cuda") for _ in self._ref_fns]
+        launcher(*gin, *gout)
+        torch.cuda.synchronize()
+        interior = tuple(slice(h, s - h) for h, s in zip(hw, shape))
+        ok = True
+        for fn, out in zip(self._ref_fns, gout):
+            params = list(inspect.signature(fn).parameters)[: -self.ndim]
+            args = [_Views(inputs.get(n, np.zeros(shape, dt)), hw) for n in params]
+            ref = array_aware(fn)(*args, *([0] * self.ndim))
+            got = out.cpu().numpy()[interior]
+            max_diff = float(np.max(np.abs(ref - got)))
+            good = bool(np.allclose(ref, got, atol=atol))
+            print(f"Validation[{fn.__name__}]: max_diff={max_diff:.2e}, pass={good}")
+            ok = ok and good
+        return ok
+
+    def benchmark(self, u_input=None, warmup: int = 5, iters: int = 20) -> dict:
+        """CUDA-event timing of ``launch_<name>`` (launcher.py:171-231); bytes
+        use the real element size."""
+        import numpy as np
+        import torch
+
+        hw = self.halo_widths
+        if u_input is None:
+            base = 128 if self.ndim == 1 else 64
+            u_np = np.random.rand(*tuple(base + 2 * h for h in hw)).astype(self._np_dtype())
+        else:
+            u_np = np.asarray(u_input, dtype=self._np_dtype())
+        launcher = getattr(self.load_module(), f"launch_{self.name}")
+        ins = [torch.from_numpy(u_np).cuda() for _ in range(max(1, len(self.inputs)))]
+        outs = [torch.zeros_like(ins[0]) for _ in range(max(1, len(self.outputs) or 1))]
+        for _ in range(warmup):
+            launcher(*ins, *outs)
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        for _ in range(iters):
+            launcher(*ins, *outs)
+        end.record()
+        end.synchronize()
+        ms = start.elapsed_time(end) / iters
+        npts = math.prod(s - 2 * h for h, s in zip(hw, u_np.shape))
+        bytes_pt = (len(ins) + len(outs)) * u_np.itemsize
+        return {"time_ms": ms, "gpoints_per_s": npts * self.temporal_steps / ms * 1e-6,
+                "gbytes_per_s": npts * bytes_pt / ms * 1e-6}
+
+
+class _Views:
+    """Offset subscripts -> shifted interior views (what ``u[i+1, j]`` means
+    when a stencil body runs on whole arrays)."""
+
+    def __init__(self, data, halo):
+        self._data = data
+        self._halo = halo
+
+    def __getitem__(self, key):
+        if not isinstance(key, tuple):
+            key = (key,)
+        sl = tuple(slice(h + k, n - h + k) for k, h, n in zip(key, self._halo, self._data.shape))
+        return self._data[sl]
+
+
+def _numpy_apply(u, fn, ndim, halo):
+    from cutile.frontend.elementwise import array_aware
+
+    res = array_aware(fn)(_Views(u, halo), *([0] * ndim))
+    out = u.copy()
+    out[tuple(slice(h, s - h) for h, s in zip(halo, u.shape))] = res
+    return out
+
+
+# --------------------------------------------------------------------------- #
+# compile()
+# --------------------------------------------------------------------------- #
+
+
+def pad_inner_halo(halo_widths: tuple[int, ...], dtype_bytes: int,
+                   align_bytes: int = 128) -> tuple[int, ...]:
+    """Round the innermost halo up to a multiple of ``align_bytes``
+    (launcher.py:257-273): 16 float64 / 32 float32 elements."""
+    if not halo_widths:
+        return halo_widths
+    align = max(1, align_bytes // dtype_bytes)
+    inner = -(-halo_widths[-1] // align) * align
+    return tuple(halo_widths[:-1]) + (inner,)
+
+
+def _num_inputs(ir) -> int:
+    from cutile.dialects.cutile_stencil.dialect import FuncOp
+
+    for op in ir.body.block.ops:
+        if isinstance(op, FuncOp):
+            return len(op.body.blocks[0].args)
+    return 1
+
+
+def _input_names(ir) -> tuple:
+    from cutile.lowering.stencil_to_target import _arg_names, _func_and_block
+
+    f, b = _func_and_block(ir)
+    return tuple(_arg_names(f, b))
+
+
+def _plan_from(tile_sizes, kernel_hints, ndim, base_plan):
+    from cutile.passes.tiling import EnginePlan
+
+    p = base_plan
+    if tile_sizes is not None:
+        t = tuple(tile_sizes)
+        if ndim == 3:
+            p = replace(p, rows=t[0], tile_y=t[1], tile_x=t[2])
+        elif ndim == 2:
+            p = replace(p, rows=t[0], tile_x=t[1])
+        else:
+            p = replace(p, tile_x=t[0])
+    if kernel_hints:
+        kw = {}
+        for k in ("threads", "stages", "zchunk"):
+            if k in kernel_hints:
+                kw[k] = int(kernel_hints[k])
+        p = replace(p, **kw)
+    assert isinstance(p, EnginePlan)
+    return p
+
+
+def generate_module_code(name: str, cuda_source: str, spec: dict, *, fused_outputs=None) -> str:
+    """Python launcher module around ``cuda_source`` (the ``code`` of a result)."""
+    from cutile.lowering.emitter import CodeEmitter
+
+    e = CodeEmitter()
+    e.line(f'"""B200 stencil module for {name} (generated)."""')
+    e.blank()
+    e.line("from cutile.runtime.module import StencilProgram")
+    e.blank()
+    e.line("CUDA_SOURCE = r'''" + cuda_source + "'''")
+    e.blank()
+    e.line(f"SPEC = {json.dumps(spec, sort_keys=True)}")
+    e.line("SPEC['halo'] = tuple(SPEC['halo'])")
+    e.line("_PROGRAM = StencilProgram(CUDA_SOURCE, SPEC)")
+    inputs = spec["input_names"]
+    outs = spec["output_params"]
+    e.blank()
+    e.blank()
+    args = ", ".join(inputs + outs)
+    e.line(f"def launch_{name}({args}, stream=None):")
+    with e.indent():
+        e.line(f'"""{spec["temporal_steps"]} step(s) of {name}; writes the interior of the output(s)."""')
+        e.line(f"_PROGRAM.launch(({', '.join(inputs)},), ({', '.join(outs)},), stream)")
+    if spec.get("boundary") is not None:
+        e.blank()
+        e.blank()
+        e.line(f"def apply_boundary_{name}(u, stream=None):")
+        with e.indent():
+            e.line('"""Apply boundary conditions to halo cells (in place)."""')
+            e.line("_PROGRAM.apply_boundary(u, stream)")
+        e.blank()
+        e.blank()
+        e.line(f"def step_{name}({args}, stream=None):")
+        with e.indent():
+            e.line('"""One step with the boundary condition fused into the staging."""')
+            e.line(f"_PROGRAM.step(({', '.join(inputs)},), ({', '.join(outs)},), stream)")
+    e.blank()
+    e.blank()
+    e.line("def program():")
+    with e.indent():
+        e.line('"""The StencilProgram behind this module."""')
+        e.line("return _PROGRAM")
+    return e.render()
+
+
+def _analysis_of(clone) -> tuple:
+    halo_widths, tile_sizes, temporal_steps = (1,), (256,), 1
+    analysis, occupancy, num_loads = {}, None, 0
+    from cutile.passes.tiling import unique_access_count
+
+    for op in clone.walk():
+        if isinstance(op, ApplyOp):
+            a = op.attributes
+            if "halo_widths" in a:
+                halo_widths = tuple(x.data for x in a["halo_widths"])
+            if "tile_sizes" in a:
+                tile_sizes = tuple(x.data for x in a["tile_sizes"])
+            if "temporal_steps" in a:
+                temporal_steps = a["temporal_steps"].data
+            if "occupancy" in a:
+                occupancy = a["occupancy"].data
+            num_loads = unique_access_count(op)
+            for key in ("flops", "unique_loads", "arithmetic_intensity", "bound"):
+                if key in a:
+                    analysis[key] = a[key].data
+            break
+    return halo_widths, tile_sizes, temporal_steps, analysis, occupancy, num_loads
+
+
+def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
+            pipeline: Pipeline | None = None, temporal_blocking: bool = True,
+            autotune: bool = True, num_gpus: int = 1, split_axis: int = 0, overlap: bool = True,
+            layout: str | None = None, brick_size: int = 32, align_halo: bool = True,
+            occupancy: int | None = None, select: str | None = None, *,
+            temporal_steps: int | None = None, tile_sizes: tuple[int, ...] | None = None,
+            kernel_hints: dict | None = None, dtype: str | None = None) -> CompileResult:
+    """Compile a ``@stencil`` function for the B200 engine (launcher.py:342-602)."""
+    from cutile.lowering.stencil_to_target import lower_to_target_ir
+    from cutile.lowering.target_to_cuda import emit_cuda
+    from cutile.passes.tiling import default_engine_plan, fit_plan
+
+    if num_gpus != 1:
+        raise NotImplementedError("multi-GPU domain decomposition is not part of the B200 backend")
+    ir = stencil_fn._ir
+    name = stencil_fn._fn.__name__
+    dtype = dtype or getattr(stencil_fn, "_dtype", "float64")
+    dtype_bytes = 4 if dtype in ("float32", "fp32") else 8
+    if hw is not None:
+        dtype_bytes = hw.dtype_bytes
+    clone = ir.clone()
+    if pipeline is None:
+        shared_mem = 49152 if hw is None else hw.shared_mem_bytes
+        pipeline = Pipeline.single_gpu(shared_mem_bytes=shared_mem, dtype_bytes=dtype_bytes,
+                                       max_temporal_steps=8 if temporal_blocking else 1)
+    pipeline.run(clone)
+    halo_widths, _ref_tile, T, analysis, pass_occ, num_loads = _analysis_of(clone)
+    if not temporal_blocking:
+        T = 1
+    num_inputs = _num_inputs(ir)
+    stencil_halo = halo_widths
+    if align_halo and layout != "bricked":
+        halo_widths = pad_inner_halo(halo_widths, dtype_bytes)
+
+    plan = default_engine_plan(len(stencil_halo), num_loads, dtype_bytes, stencil_halo, num_inputs)
+    resources = None
+    if autotune and domain is not None:
+        from cutile.runtime.autotune import autotune as _autotune
+
+        res = _autotune(stencil_fn, domain, hw=hw, dtype=dtype)
+        if res.plan is not None:
+            plan = res.plan
+        T = res.temporal_steps
+    if temporal_steps is not None:
+        T = int(temporal_steps)
+        if T > 1 and num_inputs != 1:
+            raise NotImplementedError("temporal blocking needs a single-field stencil")
+    elif num_inputs != 1:
+        # The reference's T-launch loop chains one field only
+        # (stencil_to_target.py:796-800), so a multi-field stencil cannot run
+        # blocked there either; it advances one step per launch.
+        T = 1
+    plan = _plan_from(tile_sizes, kernel_hints, len(stencil_halo), replace(plan, temporal=T))
+    plan = fit_plan(plan, stencil_halo, dtype_bytes, num_inputs)
+    hints = plan.hints()
+    if occupancy is not None:
+        hints["occupancy"] = occupancy
+
+    boundary_spec = None
+    if getattr(stencil_fn, "_boundary", None) is not None:
+        b = stencil_fn._boundary
+        boundary_spec = {"type": b} if isinstance(b, str) else (
+            dict(b) if isinstance(b, dict) else b.to_dict())
+        if "bc_type" in boundary_spec and "type" not in boundary_spec:
+            boundary_spec["type"] = boundary_spec.pop("bc_type")
+    target = lower_to_target_ir(ir.clone(), plan.tile_sizes(), halo_widths, temporal_steps=T,
+                                boundary_spec=boundary_spec, kernel_hints=hints, dtype=dtype)
+    cuda = emit_cuda(target)
+    kernels = {"main": name}
+    if boundary_spec is not None:
+        bc_plan = fit_plan(replace(plan, temporal=1), stencil_halo, dtype_bytes, num_inputs)
+        bc_target = lower_to_target_ir(ir.clone(), bc_plan.tile_sizes(), halo_widths,
+                                       temporal_steps=1, boundary_spec=boundary_spec,
+                                       kernel_hints=bc_plan.hints(), dtype=dtype,
+                                       boundary_mode=boundary_spec.get("type", "dirichlet"))
+        _rename_kernel(bc_target, f"{name}_bc")
+        cuda += "\n" + emit_cuda(bc_target, preamble=False)
+        kernels["fused_bc"] = f"{name}_bc"
+    in_names = _input_names(ir)
+    multi = num_inputs > 1
+    spec = {
+        "name": name, "ndim": len(stencil_halo), "dtype": dtype, "halo": list(halo_widths),
+        "stencil_halo": list(stencil_halo), "inputs": num_inputs, "outputs": 1,
+        "temporal_steps": T, "boundary": boundary_spec, "kernels": kernels,
+        "input_names": [n for n in "uvwxyz"][:num_inputs] if multi else ["u_in"],
+        "output_params": ["u_out"], "zchunk": plan.zchunk,
+    }
+    if multi and num_inputs > 6:
+        spec["input_names"] = [f"arr{i}" for i in range(num_inputs)]
+    code = generate_module_code(name, cuda, spec)
+    return CompileResult(
+        name=name, code=code, ndim=stencil_fn._ndim or len(halo_widths),
+        halo_widths=tuple(halo_widths), tile_sizes=plan.tile_sizes(), temporal_steps=T,
+        analysis=analysis, stencil_halo=tuple(stencil_halo), kernel_hints=hints,
+        resources=resources, inputs=in_names, cuda_source=cuda, dtype=dtype,
+        boundary=boundary_spec, layout=layout or "flat", brick_size=brick_size if layout == "bricked" else 0,
+        _ref_fn=stencil_fn._fn, _ref_fns=[stencil_fn._fn])
+
+
+def _rename_kernel(target, new_name: str) -> None:
+    from cutile.dialects.cutile_target import KernelOp
+    from cutile.ir.core import StringAttr
+
+    for op in target.body.block.ops:
+        if isinstance(op, KernelOp):
+            op.properties["kernel_name"] = StringAttr(new_name)
+
+
+# --------------------------------------------------------------------------- #
+# compile_fused()
+# --------------------------------------------------------------------------- #
+
+
+def compile_fused(stencil_fns: list, domain: tuple[int, ...] | None = None, hw=None,
+                  tile_sizes: tuple[int, ...] | None = None,
+                  halo_widths: tuple[int, ...] | None = None, temporal_steps: int = 1,
+                  occupancy: int | None = None, align_halo: bool = True,
+                  select: str | None = None, *, kernel_hints: dict | None = None,
+                  dtype: str | None = None, boundary=None) -> CompileResult:
+    """Several stencils over one domain in one multi-output kernel
+    (launcher.py:610-728): each distinct (field, offset) is staged once and
+    every output is stored.  ``boundary`` (extension) adds a ``step_<name>``
+    with that boundary condition fused into the staging of all inputs."""
+    from cutile.lowering.stencil_to_target import extract_fused_meta, lower_fused_to_target_ir
+    from cutile.lowering.target_to_cuda import emit_cuda
+    from cutile.passes.tiling import default_engine_plan, fit_plan
+
+    if not stencil_fns:
+        raise ValueError("At least one stencil function is required")
+    if temporal_steps != 1:
+        raise NotImplementedError(
+            "temporal blocking of fused kernels is not supported (temporal_steps must be 1)")
+    modules = [fn._ir for fn in stencil_fns]
+    dtype = dtype or getattr(stencil_fns[0], "_dtype", "float64")
+    meta = extract_fused_meta(modules, dtype=dtype)
+    ndim = meta.ndim
+    dtype_bytes = 4 if dtype in ("float32", "fp32") else 8
+    if hw is not None:
+        dtype_bytes = hw.dtype_bytes
+    if halo_widths is None:
+        per = []
+        for m in modules:
+            c = m.clone()
+            Pipeline.single_gpu(dtype_bytes=dtype_bytes, max_temporal_steps=1).run(c)
+            per.append(_analysis_of(c)[0])
+        halo_widths = tuple(max(hs) for hs in zip(*per)) if per else (1,) * ndim
+    stencil_halo = tuple(halo_widths)
+    if align_halo:
+        halo_widths = pad_inner_halo(tuple(halo_widths), dtype_bytes)
+    num_loads = len(meta.accesses)
+    plan = default_engine_plan(ndim, num_loads, dtype_bytes, stencil_halo, meta.num_inputs,
+                               meta.num_outputs)
+    plan = fit_plan(_plan_from(tile_sizes, kernel_hints, ndim, plan), stencil_halo, dtype_bytes,
+                    meta.num_inputs)
+    hints = plan.hints()
+    if occupancy is not None:
+        hints["occupancy"] = occupancy
+    target = lower_fused_to_target_ir(modules, plan.tile_sizes(), tuple(halo_widths), hints,
+                                      dtype=dtype)
+    cuda = emit_cuda(target)
+    kernels = {"main": meta.name}
+    bspec = None
+    if boundary is not None:
+        bspec = {"type": boundary} if isinstance(boundary, str) else (
+            dict(boundary) if isinstance(boundary, dict) else boundary.to_dict())
+        bc_target = lower_fused_to_target_ir(modules, plan.tile_sizes(), tuple(halo_widths), hints,
+                                             dtype=dtype, boundary_mode=bspec["type"])
+        _rename_kernel(bc_target, f"{meta.name}_bc")
+        cuda += "\n" + emit_cuda(bc_target, preamble=False)
+        kernels["fused_bc"] = f"{meta.name}_bc"
+    spec = {
+        "name": meta.name, "ndim": ndim, "dtype": dtype, "halo": list(halo_widths),
+        "stencil_halo": list(stencil_halo), "inputs": meta.num_inputs,
+        "outputs": meta.num_outputs, "temporal_steps": 1, "boundary": bspec, "kernels": kernels,
+        "input_names": list(meta.input_names), "output_params": meta.output_params(),
+        "zchunk": plan.zchunk,
+    }
+    code = generate_module_code(meta.name, cuda, spec)
+    return CompileResult(
+        name=meta.name, code=code, ndim=ndim, halo_widths=tuple(halo_widths),
+        tile_sizes=plan.tile_sizes(), temporal_steps=1, analysis={"unique_loads": num_loads},
+        stencil_halo=stencil_halo, kernel_hints=hints, resources=None,
+        inputs=tuple(meta.input_names), outputs=tuple(meta.output_names), cuda_source=cuda,
+        dtype=dtype, boundary=bspec, _ref_fns=[fn._fn for fn in stencil_fns],
+        _ref_inputs=meta.stencil_inputs)
+
+
+__all__ = ["compile", "compile_fused", "CompileResult", "pad_inner_halo",
+           "generate_module_code"]

@@ -1,0 +1,113 @@
+"""Runtime behind a generated stencil module.
+
+The reference's generated module is cuTile Python with ``launch_<name>``
+(stencil_to_target.py:650-843), ``apply_boundary_<name>``
+(target_to_python.py:199-297) and, for bricked layouts,
+``launch_<name>_bricked`` (multigpu_emitter.py:426-473).  Here the generated
+module is a small Python file whose functions call a ``StencilProgram``: it
+holds the CUDA source, JIT-loads it per device through libcsd, checks the
+arrays against the kernel's contract and launches on the caller's stream.
+"""
+
+from __future__ import annotations
+
+import threading
+
+from cutile.runtime import native
+
+_DTYPES = {"float64": "torch.float64", "float32": "torch.float32"}
+
+
+class StencilProgram:
+    """Launchable stencil kernels of one generated module.
+
+    ``spec`` keys: ``name``, ``ndim``, ``dtype``, ``halo`` (array halo),
+    ``stencil_halo``, ``inputs`` (count), ``outputs``, ``temporal_steps``,
+    ``boundary`` (dict or None), ``kernels`` (entry names in the source:
+    ``main`` and optionally ``fused_bc``), ``zchunk``.
+    """
+
+    def __init__(self, cuda_source: str, spec: dict):
+        self.source = cuda_source
+        self.spec = dict(spec)
+        self._modules: dict[int, native.NativeModule] = {}
+        self._lock = threading.Lock()
+
+    # -- loading -------------------------------------------------------------
+    def _module(self) -> native.NativeModule:
+        import torch
+
+        if not torch.cuda.is_available():
+            raise native.CsdError("no CUDA device: the B200 stencil backend has no CPU fallback")
+        dev = torch.cuda.current_device()
+        with self._lock:
+            m = self._modules.get(dev)
+            if m is None:
+                torch.cuda.init()
+                m = native.NativeModule(self.source)
+                self._modules[dev] = m
+        return m
+
+    def kernel(self, which: str = "main") -> native.NativeKernel:
+        return self._module().kernel(self.spec["kernels"][which])
+
+    # -- checks --------------------------------------------------------------
+    def _check(self, arrays, role: str) -> None:
+        import torch
+
+        want = torch.float64 if self.spec["dtype"] in ("float64", "fp64") else torch.float32
+        ndim = self.spec["ndim"]
+        shape = None
+        for a in arrays:
+            if not isinstance(a, torch.Tensor):
+                raise TypeError(f"{role} arrays must be torch CUDA tensors, got {type(a).__name__}")
+            if a.dtype != want:
+                raise TypeError(f"{self.spec['name']}: {role} dtype {a.dtype} does not match the "
+                                f"compiled dtype {want}")
+            if a.dim() != ndim:
+                raise ValueError(f"{self.spec['name']}: expected {ndim}-D arrays, got {a.dim()}-D")
+            if shape is None:
+                shape = tuple(a.shape)
+            elif tuple(a.shape) != shape:
+                raise ValueError(f"{self.spec['name']}: all arrays must share one shape")
+        for n, h in zip(shape, self.spec["halo"]):
+            if n - 2 * h < 1:
+                raise ValueError(f"{self.spec['name']}: extent {n} leaves no interior with halo {h}")
+
+    # -- entry points --------------------------------------------------------
+    def launch(self, inputs, outputs, stream=None, *, zchunk: int = 0, grid: int = 0,
+               loader: int = -1) -> None:
+        """``launch_<name>``: ``temporal_steps`` steps from ``inputs`` into the
+        interiors of ``outputs`` (halos untouched)."""
+        self._check(list(inputs) + list(outputs), "stencil")
+        if len(inputs) != self.spec["inputs"] or len(outputs) != self.spec["outputs"]:
+            raise TypeError(f"launch_{self.spec['name']} takes {self.spec['inputs']} input(s) and "
+                            f"{self.spec['outputs']} output(s)")
+        for o in outputs:
+            for i in inputs:
+                if o.data_ptr() == i.data_ptr():
+                    raise ValueError("outputs must not alias inputs (the kernel reads neighbours)")
+        native.launch(self.kernel("main"), inputs, outputs, self.spec["halo"], stream,
+                      zchunk=zchunk or self.spec.get("zchunk", 0), grid=grid, loader=loader)
+
+    def step(self, inputs, outputs, stream=None, **kw) -> None:
+        """One step with the declared boundary condition fused into staging:
+        ``out = stencil(apply_boundary(in))`` without writing the inputs' halos."""
+        if "fused_bc" not in self.spec["kernels"]:
+            raise ValueError(f"{self.spec['name']} declares no boundary condition")
+        self._check(list(inputs) + list(outputs), "stencil")
+        bc = self.spec["boundary"] or {}
+        native.launch(self.kernel("fused_bc"), inputs, outputs, self.spec["halo"], stream,
+                      bc_value=float(bc.get("value", 0.0)), **kw)
+
+    def apply_boundary(self, u, stream=None) -> None:
+        """``apply_boundary_<name>(u)``: fill the halo of ``u`` in place."""
+        bc = self.spec["boundary"]
+        if bc is None:
+            raise ValueError(f"{self.spec['name']} declares no boundary condition")
+        self._check([u], "boundary")
+        native.apply_boundary(u, self.spec["halo"], bc["type"], float(bc.get("value", 0.0)),
+                              stream)
+
+
+__all__ = ["StencilProgram"]

@@ -1,0 +1,253 @@
+"""ctypes binding of libcsd (the C ABI in include/csd.h).
+
+This is the only way Python reaches the GPU: every launch goes through
+``csd_launch`` / ``csd_apply_boundary`` on raw device pointers taken from
+torch tensors.  There is no CPU fallback -- if the library or a CUDA device
+is missing the calls raise.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+from pathlib import Path
+
+PKG_DIR = Path(__file__).resolve().parent.parent          # .../cutile
+ROOT_DIR = PKG_DIR.parent                                  # .../cutile-stencil-dsl_b200
+LIB_PATH = PKG_DIR / "_native" / "libcsd.so"
+INCLUDE_DIR = ROOT_DIR / "csrc" / "include"
+HEADER_NAMES = ("csd/params.h", "csd/ptx.cuh", "csd/engine.cuh")
+
+CSD_LOADER_TMA = 0
+CSD_LOADER_LDG = 1
+BC_MODES = {"none": 0, "dirichlet": 1, "neumann": 2, "periodic": 3, "reflecting": 4}
+DTYPE_CODES = {"float32": 1, "float64": 2}
+
+NVRTC_OPTIONS = (
+    "--gpu-architecture=sm_100a",
+    "-std=c++17",
+    "--fmad=false",
+    "-default-device",
+    "-DNDEBUG",
+    "-lineinfo",
+    "--ptxas-options=-v",
+)
+
+
+class CsdError(RuntimeError):
+    """A libcsd call failed; the message is ``csd_last_error()``."""
+
+
+class Field(ctypes.Structure):
+    _fields_ = [("ptr", ctypes.c_void_p), ("ndim", ctypes.c_int), ("dtype", ctypes.c_int),
+                ("shape", ctypes.c_int64 * 3), ("strides", ctypes.c_int64 * 3)]
+
+
+class LaunchOpts(ctypes.Structure):
+    _fields_ = [("halo", ctypes.c_int * 3), ("zchunk", ctypes.c_int), ("grid", ctypes.c_int),
+                ("loader", ctypes.c_int), ("bc_value", ctypes.c_double),
+                ("timeout_ns", ctypes.c_uint64)]
+
+
+class KernelDesc(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint if n == "magic" else ctypes.c_int) for n in (
+        "magic", "ndim", "nin", "nout", "dtype_bytes", "rz", "ry", "rx", "rows", "tile_y",
+        "tile_x", "vec", "threads", "stages", "nslot", "halo_chunks", "pad_left", "box_w",
+        "box_h", "smem_bytes", "zchunk", "temporal", "bc_mode", "min_blocks", "align")]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+_lib = None
+_lib_lock = threading.Lock()
+
+
+def library() -> ctypes.CDLL:
+    """Load libcsd.so (built by ``__graft_entry__.build()`` / ``make -C csrc``)."""
+    global _lib
+    with _lib_lock:
+        if _lib is not None:
+            return _lib
+        path = os.environ.get("CSD_LIBRARY", str(LIB_PATH))
+        if not os.path.exists(path):
+            raise CsdError(f"libcsd.so not found at {path}; build it with "
+                           f"`make -C {ROOT_DIR / 'csrc'}`")
+        lib = ctypes.CDLL(path)
+        P = ctypes.c_void_p
+        cp = ctypes.c_char_p
+        lib.csd_version.restype = ctypes.c_int
+        lib.csd_last_error.restype = cp
+        lib.csd_module_load.argtypes = [cp, ctypes.c_int, ctypes.POINTER(cp), ctypes.POINTER(cp), cp,
+                                        cp, ctypes.POINTER(P)]
+        lib.csd_compile.argtypes = [cp, ctypes.c_int, ctypes.POINTER(cp), ctypes.POINTER(cp), cp, cp,
+                                    ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p,
+                                    ctypes.c_size_t]
+        lib.csd_module_unload.argtypes = [P]
+        lib.csd_kernel_get.argtypes = [P, cp, ctypes.POINTER(P)]
+        lib.csd_kernel_describe.argtypes = [P, ctypes.POINTER(KernelDesc)]
+        lib.csd_kernel_resources.argtypes = [P, ctypes.POINTER(ctypes.c_int),
+                                             ctypes.POINTER(ctypes.c_int),
+                                             ctypes.POINTER(ctypes.c_int)]
+        lib.csd_launch.argtypes = [P, ctypes.POINTER(Field), ctypes.c_int, ctypes.POINTER(Field),
+                                   ctypes.c_int, ctypes.POINTER(LaunchOpts), P]
+        lib.csd_apply_boundary.argtypes = [ctypes.POINTER(Field), ctypes.POINTER(ctypes.c_int),
+                                           ctypes.c_int, ctypes.c_double, P]
+        lib.csd_error_word.argtypes = [ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+        _lib = lib
+        return lib
+
+
+def check(rc: int) -> None:
+    if rc != 0:
+        msg = library().csd_last_error().decode(errors="replace")
+        raise CsdError(f"libcsd error {rc}: {msg}")
+
+
+def _headers():
+    texts = [(INCLUDE_DIR / n).read_text() for n in HEADER_NAMES]
+    arr_t = ctypes.c_char_p * len(texts)
+    return (len(texts), arr_t(*[t.encode() for t in texts]),
+            arr_t(*[n.encode() for n in HEADER_NAMES]))
+
+
+def default_cache_dir() -> str:
+    env = os.environ.get("CSD_CACHE_DIR")
+    if env:
+        return env
+    d = ROOT_DIR / "_build" / "jit"
+    try:
+        d.mkdir(parents=True, exist_ok=True)
+        return str(d)
+    except OSError:
+        home = Path.home() / ".cache" / "cutile_b200"
+        home.mkdir(parents=True, exist_ok=True)
+        return str(home)
+
+
+def _options(extra=()) -> bytes:
+    return "\n".join(list(NVRTC_OPTIONS) + list(extra)).encode()
+
+
+def compile_source(src: str, extra_options=()) -> tuple[str, str]:
+    """NVRTC-compile a module (no GPU needed); returns (cubin path, log)."""
+    lib = library()
+    n, hdrs, names = _headers()
+    path = ctypes.create_string_buffer(4096)
+    log = ctypes.create_string_buffer(1 << 16)
+    check(lib.csd_compile(src.encode(), n, hdrs, names, _options(extra_options),
+                          default_cache_dir().encode(), path, 4096, log, 1 << 16))
+    return path.value.decode(), log.value.decode(errors="replace")
+
+
+class NativeModule:
+    """A loaded JIT module (per CUDA context)."""
+
+    def __init__(self, src: str, extra_options=()):
+        lib = library()
+        n, hdrs, names = _headers()
+        handle = ctypes.c_void_p()
+        check(lib.csd_module_load(src.encode(), n, hdrs, names, _options(extra_options),
+                                  default_cache_dir().encode(), ctypes.byref(handle)))
+        self.handle = handle
+        self._kernels: dict[str, NativeKernel] = {}
+
+    def kernel(self, name: str) -> "NativeKernel":
+        k = self._kernels.get(name)
+        if k is None:
+            handle = ctypes.c_void_p()
+            check(library().csd_kernel_get(self.handle, name.encode(), ctypes.byref(handle)))
+            k = NativeKernel(name, handle)
+            self._kernels[name] = k
+        return k
+
+
+class NativeKernel:
+    def __init__(self, name: str, handle: ctypes.c_void_p):
+        self.name = name
+        self.handle = handle
+        d = KernelDesc()
+        check(library().csd_kernel_describe(handle, ctypes.byref(d)))
+        self.desc = d.as_dict()
+
+    def resources(self) -> dict:
+        regs, local, blocks = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(library().csd_kernel_resources(self.handle, ctypes.byref(regs), ctypes.byref(local),
+                                             ctypes.byref(blocks)))
+        return {"registers": regs.value, "local_bytes": local.value,
+                "blocks_per_sm": blocks.value}
+
+
+def field_of(t) -> Field:
+    """csd_field for a torch tensor (must be on CUDA, float32/float64, contiguous)."""
+    import torch
+
+    if not isinstance(t, torch.Tensor):
+        raise TypeError(f"expected a torch.Tensor, got {type(t).__name__}")
+    if not t.is_cuda:
+        raise ValueError("stencil fields must be CUDA tensors")
+    if t.dtype == torch.float64:
+        code = 2
+    elif t.dtype == torch.float32:
+        code = 1
+    else:
+        raise TypeError(f"unsupported dtype {t.dtype}")
+    if t.dim() < 1 or t.dim() > 3:
+        raise ValueError("fields must be 1-, 2- or 3-D")
+    if not t.is_contiguous():
+        raise ValueError("fields must be C-contiguous")
+    f = Field()
+    f.ptr = t.data_ptr()
+    f.ndim = t.dim()
+    f.dtype = code
+    for i in range(t.dim()):
+        f.shape[i] = t.shape[i]
+        f.strides[i] = t.stride(i)
+    return f
+
+
+def stream_handle(stream) -> int | None:
+    import torch
+
+    if stream is None:
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, int):
+        return stream
+    return getattr(stream, "cuda_stream", None) or getattr(stream, "ptr", None)
+
+
+def launch(kernel: NativeKernel, inputs, outputs, halo, stream=None, *, zchunk: int = 0,
+           grid: int = 0, loader: int = -1, bc_value: float = 0.0, timeout_ns: int = 0) -> None:
+    lib = library()
+    fin = (Field * len(inputs))(*[field_of(t) for t in inputs])
+    fout = (Field * len(outputs))(*[field_of(t) for t in outputs])
+    o = LaunchOpts()
+    for i, h in enumerate(halo):
+        o.halo[i] = int(h)
+    o.zchunk = zchunk
+    o.grid = grid
+    o.loader = loader
+    o.bc_value = bc_value
+    o.timeout_ns = timeout_ns
+    check(lib.csd_launch(kernel.handle, fin, len(inputs), fout, len(outputs), ctypes.byref(o),
+                         ctypes.c_void_p(stream_handle(stream))))
+
+
+def apply_boundary(t, halo, bc: str, value: float = 0.0, stream=None) -> None:
+    lib = library()
+    f = field_of(t)
+    h = (ctypes.c_int * 3)(*([int(x) for x in halo] + [0] * (3 - len(halo))))
+    check(lib.csd_apply_boundary(ctypes.byref(f), h, BC_MODES[bc], float(value),
+                                 ctypes.c_void_p(stream_handle(stream))))
+
+
+def error_word(reset: bool = True) -> int:
+    v = ctypes.c_int()
+    check(library().csd_error_word(ctypes.byref(v), 1 if reset else 0))
+    return v.value
+
+
+__all__ = ["library", "check", "compile_source", "NativeModule", "NativeKernel", "launch",
+           "apply_boundary", "error_word", "CsdError", "field_of", "default_cache_dir",
+           "CSD_LOADER_TMA", "CSD_LOADER_LDG", "BC_MODES"]

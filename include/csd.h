@@ -1,0 +1,121 @@
+/*
+ * csd.h -- C ABI of the B200 stencil backend (libcsd.so).
+ *
+ * The reference (cutile-stencil-dsl) has no native boundary: its generated
+ * module is Python that calls cuTile (`ct.launch`, emitted by
+ * cutile/lowering/target_to_python.py:356-399) and CuPy slice copies for
+ * boundaries (target_to_python.py:199-297).  This header is the boundary
+ * that replaces those calls.  Each entry point cites the reference interface
+ * it stands in for; INTEGRATION.md shows how a caller binds it.
+ *
+ * Conventions: every function returns 0 on success or a CSD_E* code; the
+ * message of the last failure on the calling thread is csd_last_error().
+ * Arrays are C-contiguous device buffers described by csd_field; strides
+ * are in elements.  Launches are asynchronous on the given CUDA stream
+ * (NULL = the legacy default stream) and allocate nothing per call.
+ */
+#ifndef CSD_H
+#define CSD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../cutile-stencil-dsl_b200/csrc/include/csd/params.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CSD_OK 0
+#define CSD_EINVAL 1      /* invalid argument (shape, dtype, count) */
+#define CSD_EALIGN 2      /* misaligned pointer or pitch for the requested path */
+#define CSD_ECOMPILE 3    /* NVRTC compilation failed (log in csd_last_error) */
+#define CSD_ELAUNCH 4     /* CUDA driver / launch failure */
+#define CSD_ETIMEOUT 5    /* a kernel gave up waiting (device error word set) */
+#define CSD_ENODEV 6      /* no CUDA driver or device */
+#define CSD_ENOSYM 7      /* kernel or descriptor missing from a module */
+
+#define CSD_DTYPE_F32 1
+#define CSD_DTYPE_F64 2
+
+typedef struct csd_module csd_module;
+typedef struct csd_kernel csd_kernel;
+
+/* One array argument: C-contiguous, `ndim` dims, sizes in `shape`. */
+typedef struct csd_field {
+  void* ptr;
+  int ndim;
+  int dtype;            /* CSD_DTYPE_* */
+  int64_t shape[3];
+  int64_t strides[3];   /* elements; must describe a C-contiguous layout */
+} csd_field;
+
+/* Per-launch options (zero-initialise for defaults). */
+typedef struct csd_launch_opts {
+  int halo[3];          /* array halo width per array dim (interior = shape - 2*halo) */
+  int zchunk;           /* output rows per work item along dim 0 (0 = kernel default) */
+  int grid;             /* persistent CTAs (0 = occupancy x SM count) */
+  int loader;           /* -1 auto, CSD_LOADER_TMA, CSD_LOADER_LDG */
+  double bc_value;      /* Dirichlet value when the kernel fuses a boundary fill */
+  uint64_t timeout_ns;  /* bound on device waits (0 = 2 s) */
+} csd_launch_opts;
+
+/* Library version (major*100 + minor). */
+int csd_version(void);
+
+/* Message of the last error on this thread ("" if none). */
+const char* csd_last_error(void);
+
+/* Compile `src` (CUDA C++ of a generated stencil module) for sm_100a with
+ * NVRTC, caching the cubin under `cache_dir` (NULL: no disk cache), and load
+ * it into the current device's primary context.  `headers`/`header_names`
+ * provide the engine headers the source includes.  Replaces cuTile's JIT of
+ * the generated module at first launch (reference: README.md:487-492,
+ * runtime/launcher.py:62-74 `load_module`). */
+int csd_module_load(const char* src, int n_headers, const char* const* headers,
+                    const char* const* header_names, const char* options,
+                    const char* cache_dir, csd_module** out);
+
+/* Compile only (no device needed): writes the cubin path into `cubin_path`
+ * (buffer of `path_len` bytes) and the NVRTC log (ptxas -v) into `log`. */
+int csd_compile(const char* src, int n_headers, const char* const* headers,
+                const char* const* header_names, const char* options, const char* cache_dir,
+                char* cubin_path, size_t path_len, char* log, size_t log_len);
+
+int csd_module_unload(csd_module* m);
+
+/* Look up stencil kernel `name` (its `<name>_tma`, `<name>_ldg` entry points
+ * and `<name>_desc` descriptor).  Stands in for the generated
+ * `<name>_kernel` object (target_to_python.py:34-191). */
+int csd_kernel_get(csd_module* m, const char* name, csd_kernel** out);
+
+/* Copy the kernel's compile-time descriptor. */
+int csd_kernel_describe(const csd_kernel* k, csd_kernel_desc* out);
+
+/* Registers per thread, local (spill) bytes per thread and resident blocks
+ * per SM of the TMA variant.  Replaces the reference's cubin probe
+ * (runtime/regcheck.py:136-212) with driver attributes. */
+int csd_kernel_resources(csd_kernel* k, int* regs, int* local_bytes, int* blocks_per_sm);
+
+/* One stencil pass: read `in[0..n_in)`, write the interior of
+ * `out[0..n_out)`.  Equivalent of `launch_<name>(inputs..., outputs...)`
+ * (stencil_to_target.py:677-843): `temporal` steps per call for chained
+ * kernels, output halos untouched. */
+int csd_launch(csd_kernel* k, const csd_field* in, int n_in, const csd_field* out, int n_out,
+               const csd_launch_opts* opts, void* stream);
+
+/* Fill the halo of `f` in place with boundary condition `bc` (CSD_BC_*),
+ * dimension by dimension.  Equivalent of `apply_boundary_<name>(u)`
+ * (target_to_python.py:199-297) and stencil_ref.apply_boundary
+ * (reference/stencil_ref.py:102-201). */
+int csd_apply_boundary(const csd_field* f, const int* halo, int bc, double value, void* stream);
+
+/* Read (and with reset != 0, clear) the device error word of the current
+ * device; synchronises the device. */
+int csd_error_word(int* value, int reset);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CSD_H */
