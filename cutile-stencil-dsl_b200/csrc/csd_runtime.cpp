@@ -501,7 +501,9 @@ int csd_launch(csd_kernel* k, const csd_field* in, int n_in, const csd_field* ou
   memset(&p, 0, sizeof(p));
   int halo[3];
   view3(f0, p.dims, o.halo, halo);
-  const int rad[3] = {D.rz, D.ry, D.rx};
+  // per-step radius: chained steps see zero halos beyond the interior, so the
+  // array needs only one step's halo
+  const int rad[3] = {D.rz / D.temporal, D.ry / D.temporal, D.rx / D.temporal};
   for (int d = 0; d < 3; ++d) {
     p.halo[d] = halo[d];
     p.interior[d] = (int)(p.dims[d] - 2 * halo[d]);

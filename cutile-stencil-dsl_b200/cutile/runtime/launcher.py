@@ -276,7 +276,7 @@ def generate_module_code(name: str, cuda_source: str, spec: dict, *, fused_outpu
     e.blank()
     e.line("CUDA_SOURCE = r'''" + cuda_source + "'''")
     e.blank()
-    e.line(f"SPEC = {json.dumps(spec, sort_keys=True)}")
+    e.line(f"SPEC = {spec!r}")
     e.line("SPEC['halo'] = tuple(SPEC['halo'])")
     e.line("_PROGRAM = StencilProgram(CUDA_SOURCE, SPEC)")
     inputs = spec["input_names"]
