@@ -341,7 +341,10 @@ def main() -> None:
     ap.add_argument("--dtype", choices=("float64", "float32"), default="float64")
     ap.add_argument("--temporal", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--n", type=int, default=512, help="interior extent per dimension")
     args = ap.parse_args()
+    global N_INTERIOR
+    N_INTERIOR = args.n
     if args.warmup < 3:
         args.warmup = 3
     line = run_reference(args) if args.impl == "reference" else run_ours(args)
