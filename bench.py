@@ -278,7 +278,7 @@ def _slab_job(args):
     return time.perf_counter() - t0, nz * N_INTERIOR * N_INTERIOR * steps
 
 
-def cpu_baseline(np_dtype, cores: int = 1, planes: int = 48, steps: int = 4) -> dict:
+def cpu_baseline(np_dtype, cores: int = 1, planes: int = 96, steps: int = 20) -> dict:
     """The oracle (NumPy restatement of reference/stencil_ref.apply_stencil)
     on z-slabs of the 512^2 cross-section, ``cores`` worker processes."""
     import multiprocessing as mp

@@ -104,3 +104,135 @@ extern "C" int csd_apply_boundary(const csd_field* f, const int* halo, int bc, d
   if (f->dtype == CSD_DTYPE_F32) return apply_boundary_t<float>(f, halo, bc, value, s);
   return csd_internal_fail(CSD_EINVAL, "unsupported dtype");
 }
+
+// ---------------------------------------------------------------------------
+// FP64 reductions over the interior of a field (mass, energy, residual, max)
+//
+// Deterministic: pass 1 gives CTA b the interior rows [b*R/G, (b+1)*R/G) of
+// the (Z*Y) x X row grid; each thread accumulates its elements in a fixed
+// order in FP64, then a fixed-shape tree reduces the CTA's threads into
+// partials[b].  Pass 2 (one CTA) reduces partials[0..G) the same way.  The
+// result depends on G, never on scheduling.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int RED_THREADS = 256;
+
+template <int OP>
+__device__ __forceinline__ double red_combine(double a, double b) {
+  if (OP == CSD_RED_MAXABS || OP == CSD_RED_DIFF_MAXABS) return (a != a || a > b) ? a : b;
+  return a + b;
+}
+
+template <int OP>
+__device__ __forceinline__ double red_block(double v, double* sh) {
+  // fixed-shape tree: warp shuffles, then the warp totals in order
+  for (int o = 16; o > 0; o >>= 1) v = red_combine<OP>(v, __shfl_down_sync(0xffffffffu, v, o));
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) sh[warp] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0) {
+    t = sh[0];
+    for (int w = 1; w < RED_THREADS / 32; ++w) t = red_combine<OP>(t, sh[w]);
+  }
+  __syncthreads();
+  return t;
+}
+
+template <typename T, int OP>
+__global__ void __launch_bounds__(RED_THREADS) reduce_pass1(const T* a, const T* b, long long d0,
+                                                            long long d1, long long d2, int h0,
+                                                            int h1, int h2, double* partials) {
+  __shared__ double sh[RED_THREADS / 32];
+  const long long ny = d1 - 2 * h1, nx = d2 - 2 * h2;
+  const long long rows = (d0 - 2 * h0) * ny;
+  const long long r0 = rows * blockIdx.x / gridDim.x, r1 = rows * (blockIdx.x + 1) / gridDim.x;
+  double acc = 0.0;
+  for (long long r = r0; r < r1; ++r) {
+    const long long z = r / ny + h0, y = r % ny + h1;
+    const long long base = (z * d1 + y) * d2 + h2;
+    for (long long x = threadIdx.x; x < nx; x += RED_THREADS) {
+      const double va = (double)a[base + x];
+      double v;
+      if (OP == CSD_RED_SUM) v = va;
+      else if (OP == CSD_RED_SUMSQ) v = va * va;
+      else if (OP == CSD_RED_MAXABS) v = fabs(va);
+      else {
+        const double d = va - (double)b[base + x];
+        v = (OP == CSD_RED_DIFF_SUMSQ) ? d * d : fabs(d);
+      }
+      acc = red_combine<OP>(acc, v);
+    }
+  }
+  const double t = red_block<OP>(acc, sh);
+  if (threadIdx.x == 0) partials[blockIdx.x] = t;
+}
+
+template <int OP>
+__global__ void __launch_bounds__(RED_THREADS) reduce_pass2(const double* partials, int n,
+                                                            double* result) {
+  __shared__ double sh[RED_THREADS / 32];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += RED_THREADS) acc = red_combine<OP>(acc, partials[i]);
+  const double t = red_block<OP>(acc, sh);
+  if (threadIdx.x == 0) *result = t;
+}
+
+template <typename T, int OP>
+int reduce_t(const csd_field* a, const csd_field* b, const long long d[3], const int h[3],
+             double* partials, int nblocks, double* result, cudaStream_t s) {
+  const T* pa = reinterpret_cast<const T*>(a->ptr);
+  const T* pb = b ? reinterpret_cast<const T*>(b->ptr) : nullptr;
+  reduce_pass1<T, OP><<<nblocks, RED_THREADS, 0, s>>>(pa, pb, d[0], d[1], d[2], h[0], h[1], h[2],
+                                                      partials);
+  reduce_pass2<OP><<<1, RED_THREADS, 0, s>>>(partials, nblocks, result);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? CSD_OK : csd_internal_fail(CSD_ELAUNCH, cudaGetErrorString(e));
+}
+
+template <typename T>
+int reduce_dispatch(int op, const csd_field* a, const csd_field* b, const long long d[3],
+                    const int h[3], double* partials, int nblocks, double* result,
+                    cudaStream_t s) {
+  switch (op) {
+    case CSD_RED_SUM: return reduce_t<T, CSD_RED_SUM>(a, b, d, h, partials, nblocks, result, s);
+    case CSD_RED_SUMSQ: return reduce_t<T, CSD_RED_SUMSQ>(a, b, d, h, partials, nblocks, result, s);
+    case CSD_RED_MAXABS: return reduce_t<T, CSD_RED_MAXABS>(a, b, d, h, partials, nblocks, result, s);
+    case CSD_RED_DIFF_SUMSQ:
+      return reduce_t<T, CSD_RED_DIFF_SUMSQ>(a, b, d, h, partials, nblocks, result, s);
+    case CSD_RED_DIFF_MAXABS:
+      return reduce_t<T, CSD_RED_DIFF_MAXABS>(a, b, d, h, partials, nblocks, result, s);
+  }
+  return csd_internal_fail(CSD_EINVAL, "unknown reduction");
+}
+
+}  // namespace
+
+extern "C" int csd_reduce(const csd_field* a, const csd_field* b, const int* halo, int op,
+                          double* partials, int nblocks, double* result, void* stream) {
+  if (!a || !a->ptr || !halo || !partials || !result || nblocks < 1)
+    return csd_internal_fail(CSD_EINVAL, "null argument or nblocks < 1");
+  if (a->ndim < 1 || a->ndim > 3) return csd_internal_fail(CSD_EINVAL, "ndim must be 1-3");
+  const bool diff = (op == CSD_RED_DIFF_SUMSQ || op == CSD_RED_DIFF_MAXABS);
+  if (diff) {
+    if (!b || !b->ptr || b->dtype != a->dtype || b->ndim != a->ndim)
+      return csd_internal_fail(CSD_EINVAL, "difference reductions need a second field like the first");
+    for (int i = 0; i < a->ndim; ++i)
+      if (b->shape[i] != a->shape[i]) return csd_internal_fail(CSD_EINVAL, "field shapes differ");
+  }
+  long long d[3] = {1, 1, 1};
+  int h[3] = {0, 0, 0};
+  const int off = 3 - a->ndim;
+  for (int i = 0; i < a->ndim; ++i) {
+    d[off + i] = a->shape[i];
+    h[off + i] = halo[i];
+    if (d[off + i] - 2 * h[off + i] < 1) return csd_internal_fail(CSD_EINVAL, "empty interior");
+  }
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (a->dtype == CSD_DTYPE_F64)
+    return reduce_dispatch<double>(op, a, diff ? b : nullptr, d, h, partials, nblocks, result, s);
+  if (a->dtype == CSD_DTYPE_F32)
+    return reduce_dispatch<float>(op, a, diff ? b : nullptr, d, h, partials, nblocks, result, s);
+  return csd_internal_fail(CSD_EINVAL, "unsupported dtype");
+}

@@ -519,8 +519,21 @@ int csd_launch(csd_kernel* k, const csd_field* in, int n_in, const csd_field* ou
   p.xbase = (p.halo[2] / D.align) * D.align;
   p.tiles[0] = (p.halo[2] + p.interior[2] - p.xbase + D.tile_x - 1) / D.tile_x;
   p.tiles[1] = (p.interior[1] + D.tile_y - 1) / D.tile_y;
-  p.zchunk = o.zchunk > 0 ? o.zchunk : D.zchunk;
-  p.zchunk = ((p.zchunk + D.rows - 1) / D.rows) * D.rows;
+  // Persistent CTAs that fit at once; the work items (column tiles x Z
+  // chunks) are sized so that they fill these slots in one wave: items of
+  // equal length that start together keep neighbouring columns on the same
+  // planes (their halo rows are then shared in L2) and leave no tail.
+  int loader_guess = o.loader == CSD_LOADER_LDG ? CSD_LOADER_LDG : CSD_LOADER_TMA;
+  const long long slots = o.grid > 0 ? o.grid : (long long)k->blocks_per_sm[loader_guess] * st->sms;
+  const long long columns = (long long)p.tiles[0] * p.tiles[1];
+  int zchunk = o.zchunk > 0 ? o.zchunk : D.zchunk;
+  if (zchunk <= 0) {
+    long long nzc = slots / (columns > 0 ? columns : 1);
+    if (nzc < 1) nzc = 1;
+    if (nzc > p.interior[0]) nzc = p.interior[0];
+    zchunk = (int)((p.interior[0] + nzc - 1) / nzc);
+  }
+  p.zchunk = ((zchunk + D.rows - 1) / D.rows) * D.rows;
   if (p.zchunk > p.interior[0]) p.zchunk = ((p.interior[0] + D.rows - 1) / D.rows) * D.rows;
   p.tiles[2] = (p.interior[0] + p.zchunk - 1) / p.zchunk;
   long long items = (long long)p.tiles[0] * p.tiles[1] * p.tiles[2];

@@ -88,7 +88,7 @@ class StencilProgram:
                 if o.data_ptr() == i.data_ptr():
                     raise ValueError("outputs must not alias inputs (the kernel reads neighbours)")
         native.launch(self.kernel("main"), inputs, outputs, self.spec["halo"], stream,
-                      zchunk=zchunk or self.spec.get("zchunk", 0), grid=grid, loader=loader)
+                      zchunk=zchunk, grid=grid, loader=loader)
 
     def step(self, inputs, outputs, stream=None, **kw) -> None:
         """One step with the declared boundary condition fused into staging:

@@ -95,6 +95,9 @@ def library() -> ctypes.CDLL:
         lib.csd_apply_boundary.argtypes = [ctypes.POINTER(Field), ctypes.POINTER(ctypes.c_int),
                                            ctypes.c_int, ctypes.c_double, P]
         lib.csd_error_word.argtypes = [ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+        lib.csd_reduce.argtypes = [ctypes.POINTER(Field), ctypes.POINTER(Field),
+                                   ctypes.POINTER(ctypes.c_int), ctypes.c_int, P, ctypes.c_int, P,
+                                   P]
         _lib = lib
         return lib
 

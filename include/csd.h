@@ -110,6 +110,21 @@ int csd_launch(csd_kernel* k, const csd_field* in, int n_in, const csd_field* ou
  * (reference/stencil_ref.py:102-201). */
 int csd_apply_boundary(const csd_field* f, const int* halo, int bc, double value, void* stream);
 
+#define CSD_RED_SUM 0         /* mass:      sum(a) */
+#define CSD_RED_SUMSQ 1       /* energy:    sum(a^2) */
+#define CSD_RED_MAXABS 2      /* max |a| (NaN propagates) */
+#define CSD_RED_DIFF_SUMSQ 3  /* residual:  sum((a-b)^2) */
+#define CSD_RED_DIFF_MAXABS 4 /* max |a-b| */
+
+/* FP64 reduction over the interior of `a` (and `b` for the DIFF ops),
+ * deterministic for a given `nblocks`: pass 1 writes one partial per block
+ * into the caller's device scratch `partials[nblocks]`, pass 2 writes the
+ * total to the device double `*result`.  No reference counterpart: the
+ * reference reduces on the host with NumPy (e.g. examples/shallow_water.py
+ * energy); the B200 path keeps these global sums on the device in FP64. */
+int csd_reduce(const csd_field* a, const csd_field* b, const int* halo, int op,
+               double* partials, int nblocks, double* result, void* stream);
+
 /* Read (and with reset != 0, clear) the device error word of the current
  * device; synchronises the device. */
 int csd_error_word(int* value, int reset);
