@@ -236,3 +236,63 @@ extern "C" int csd_reduce(const csd_field* a, const csd_field* b, const int* hal
     return reduce_dispatch<float>(op, a, diff ? b : nullptr, d, h, partials, nblocks, result, s);
   return csd_internal_fail(CSD_EINVAL, "unsupported dtype");
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free reduction entry point.
+//
+// For callers that must not allocate device memory themselves: a host
+// process whose device memory is entirely owned by another allocator (a
+// framework's caching pool, a fixed up-front reservation), or a loop that
+// cannot afford cudaMalloc's implicit device synchronisation between steps.
+// They cannot provide the `partials` scratch csd_reduce needs, so this
+// variant keeps its per-block partials in a file-scope device array of fixed
+// size, which every device holds from the moment the library's kernels load
+// until the process exits.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace {
+
+// One partial per block of pass 1 (8 KB).  Shared by every call: pass 1
+// overwrites each of the `nblocks` entries it uses before pass 2 reads them,
+// so nothing has to be cleared between calls, but two calls that run at the
+// same time on the GPU (different streams) race on these entries.
+static __device__ __align__(256) double g_noalloc_partials[CSD_NOALLOC_MAX_BLOCKS];
+
+// Device address of g_noalloc_partials per device ordinal (the host-side
+// name is only a stand-in for the symbol, never a device pointer).
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[64] = {nullptr};
+
+int noalloc_scratch(double** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return csd_internal_fail(CSD_ENODEV, cudaGetErrorString(e));
+  if (dev < 0 || dev >= 64) return csd_internal_fail(CSD_EINVAL, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+    if (e != cudaSuccess)
+      return csd_internal_fail(CSD_ELAUNCH, cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = static_cast<double*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return CSD_OK;
+}
+
+}  // namespace
+
+extern "C" int csd_reduce_noalloc(const csd_field* a, const csd_field* b, const int* halo, int op,
+                                  int nblocks, double* result, void* stream) {
+  if (nblocks < 1 || nblocks > CSD_NOALLOC_MAX_BLOCKS)
+    return csd_internal_fail(CSD_EINVAL,
+                             "csd_reduce_noalloc: nblocks must be 1..1024 (the static scratch "
+                             "holds 1024 partials)");
+  if (!a || !a->ptr || !halo || !result)
+    return csd_internal_fail(CSD_EINVAL, "csd_reduce_noalloc: null argument");
+  double* partials = nullptr;
+  int rc = noalloc_scratch(&partials);
+  if (rc) return rc;
+  return csd_reduce(a, b, halo, op, partials, nblocks, result, stream);
+}

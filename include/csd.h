@@ -125,6 +125,21 @@ int csd_apply_boundary(const csd_field* f, const int* halo, int bc, double value
 int csd_reduce(const csd_field* a, const csd_field* b, const int* halo, int op,
                double* partials, int nblocks, double* result, void* stream);
 
+/* csd_reduce without caller-provided scratch, for callers that cannot
+ * allocate device memory (their device memory belongs to another allocator,
+ * or a step loop must not pay cudaMalloc's device synchronisation).  The
+ * per-block partials live in a file-scope device array of
+ * CSD_NOALLOC_MAX_BLOCKS = 1024 doubles (8 KB) that every device keeps until
+ * the process exits; `nblocks` above 1024 is rejected with CSD_EINVAL.  The
+ * first call on a device looks up the array's device address (with that
+ * device current); make that first call before any stream capture.  Calls
+ * share the array, so calls that overlap on the GPU race; each call
+ * overwrites the partials it uses, so no clearing is needed.  Nothing is
+ * allocated.  No counterpart in the reference. */
+#define CSD_NOALLOC_MAX_BLOCKS 1024
+int csd_reduce_noalloc(const csd_field* a, const csd_field* b, const int* halo, int op,
+                       int nblocks, double* result, void* stream);
+
 /* Read (and with reset != 0, clear) the device error word of the current
  * device; synchronises the device. */
 int csd_error_word(int* value, int reset);
