@@ -100,6 +100,7 @@ class Program:
         self.result_type: str = "w"
         self.expression: str = ""
         self.access_uses: dict[int, int] = {}
+        self.extra_returns: list[tuple[str, int]] = []
 
 
 def build_program(block, access_index: dict, field_dtype: str, spatial_order: bool = False,
@@ -310,3 +311,46 @@ def _rebuild_sum(prog, terms, operand, text, vtype, new, const):
 
 
 __all__ = ["Program", "build_program", "_f32_exact"]
+
+
+def kahan_rewrite(prog: Program, center_access: dict, comp_access: int, out_index: int,
+                  comp_out_index: int) -> int:
+    """Turn a ``u + incr`` program into a Kahan-compensated FP32 update.
+
+    ``center_access`` maps access indices that read a field at offset zero to
+    that field; ``comp_access`` is the access index of the compensation field.
+    The program's final ``addf`` (either operand order) must add a center read
+    to the increment.  Returns the array index of the updated field.  The new
+    tail is (all float32, round-to-nearest, no contraction)::
+
+        y  = incr - c          t  = u + y
+        c' = (t - u) - y       outputs: t -> out_index, c' -> comp_out_index
+    """
+    last = prog.lines[-1]
+    lhs, rhs = last.split(" = ", 1)
+    body, typ = rhs.rsplit(" : ", 1)
+    if lhs != prog.result or not body.startswith("addf "):
+        raise ValueError("Kahan-compensated updates need a body of the form `u + increment`")
+    a, b = [t.strip() for t in body[5:].split(",")]
+    def center(tok):
+        return tok.startswith("a") and tok[1:].isdigit() and int(tok[1:]) in center_access
+    if center(a):
+        u, incr = a, b
+    elif center(b):
+        u, incr = b, a
+    else:
+        raise ValueError("Kahan-compensated updates need a body of the form `u[i, j] + increment`")
+    field = center_access[int(u[1:])]
+    lines = prog.lines[:-1]
+    c = f"a{comp_access}"
+    lines.append(f"k0 = cast {incr} : f32")
+    lines.append(f"k1 = subf k0, {c} : f32")
+    lines.append(f"k2 = addf {u}, k1 : f32")
+    lines.append(f"k3 = subf k2, {u} : f32")
+    lines.append(f"k4 = subf k3, k1 : f32")
+    prog.lines = lines
+    prog.result = "k2"
+    prog.result_type = "f32"
+    prog.extra_returns = [("k2", out_index), ("k4", comp_out_index)]
+    prog.expression = f"kahan({prog.expression})"
+    return field

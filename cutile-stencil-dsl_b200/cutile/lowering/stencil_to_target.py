@@ -41,7 +41,7 @@ from cutile.ir.core import (
     Region,
     StringAttr,
 )
-from cutile.lowering.expr import Program, build_program
+from cutile.lowering.expr import Program, build_program, kahan_rewrite
 
 _IDX = IndexType()
 
@@ -79,10 +79,11 @@ class _StencilMeta:
         self.output_names: list[str] = []
         self.stencil_inputs: list[list[str]] = []
         self.programs: list[Program] = []
+        self.kahan = False
 
     @property
     def num_outputs(self) -> int:
-        return max(1, len(self.expressions))
+        return max(1, len(self.expressions)) * (2 if self.kahan else 1)
 
     def output_views(self) -> list[str]:
         if self.num_outputs == 1:
@@ -91,8 +92,9 @@ class _StencilMeta:
 
     def output_params(self) -> list[str]:
         if self.output_names:
-            return [f"{n}_out" for n in self.output_names]
-        return ["u_out"]
+            outs = [f"{n}_out" for n in self.output_names]
+            return outs + [f"{n}_c_out" for n in self.output_names] if self.kahan else outs
+        return ["u_out", "c_out"] if self.kahan else ["u_out"]
 
     def halo(self) -> tuple[int, ...]:
         """Stencil footprint per dimension (max |offset|)."""
@@ -283,6 +285,34 @@ def extract_fused_meta(modules: Sequence[ModuleOp], spatial_term_order: bool | N
     return fused
 
 
+def apply_kahan(meta: _StencilMeta, comp_names: Sequence[str] | None = None) -> _StencilMeta:
+    """Rewrite every output of *meta* as a Kahan-compensated FP32 update.
+
+    Each program must compute ``u + increment`` with ``u`` a zero-offset read
+    of one input field; a compensation field per output is appended to the
+    inputs (``c_<field>``) and a compensation output to the outputs.
+    """
+    if meta.dtype not in ("float32", "fp32"):
+        raise ValueError("Kahan-compensated updates are an FP32 mode (dtype float32)")
+    m_count = len(meta.programs)
+    center = {j: a.array_index for j, a in enumerate(meta.accesses) if not any(a.offsets)}
+    zeros = (0,) * meta.ndim
+    for m, prog in enumerate(meta.programs):
+        name = f"c{len(meta.input_names)}"
+        meta.input_names.append(name)
+        j = len(meta.accesses)
+        meta.accesses.append(_AccessInfo(len(meta.input_names) - 1, zeros, f"{name}_0_0"))
+        field = kahan_rewrite(prog, center, j, m, m_count + m)
+        meta.input_names[-1] = (comp_names[m] if comp_names else
+                                f"c_{meta.input_names[field]}")
+        meta.accesses[j].view_name = f"{meta.input_names[-1]}_0_0"
+    meta.num_inputs = len(meta.input_names)
+    meta.kahan = True
+    meta.expressions = [p.expression for p in meta.programs]
+    meta.expression = meta.expressions[0]
+    return meta
+
+
 def _owners(shared, metas):
     done = set()
     for m in metas:
@@ -351,7 +381,9 @@ def _build_kernel_op(meta: _StencilMeta, tile_sizes: tuple[int, ...], halo_width
             ArrayAttr([IntAttr(a.array_index)] + [IntAttr(o) for o in a.offsets])
             for a in meta.accesses]),
         "ssa_body": ArrayAttr([
-            ArrayAttr([StringAttr(line) for line in p.lines] + [StringAttr(f"return {p.result}")])
+            ArrayAttr([StringAttr(line) for line in p.lines] + (
+                [StringAttr(f"return {v} @{i}") for v, i in p.extra_returns]
+                if p.extra_returns else [StringAttr(f"return {p.result}")]))
             for p in meta.programs]),
         "temporal_steps": IntAttr(temporal_steps),
         "layout": StringAttr(layout),
@@ -412,10 +444,12 @@ def lower_to_target_ir(module: ModuleOp, tile_sizes: tuple[int, ...], halo_width
                        temporal_steps: int = 1, boundary_spec: dict | None = None,
                        kernel_hints: dict | None = None, spatial_term_order: bool | None = None,
                        *, dtype: str | None = None, layout: str = "flat", brick_size: int = 0,
-                       boundary_mode: str = "none") -> ModuleOp:
+                       boundary_mode: str = "none", kahan: bool = False) -> ModuleOp:
     """Dialect 1 module -> Dialect 3 module (``cutile.kernel`` + host program)."""
     func_op, block = _func_and_block(module)
     meta = _extract_meta(func_op, block, spatial_term_order, dtype=dtype)
+    if kahan:
+        apply_kahan(meta)
     if boundary_spec is None and meta.boundary is not None:
         boundary_spec = meta.boundary
     kernel = _build_kernel_op(meta, tile_sizes, halo_widths, kernel_hints,
@@ -437,8 +471,10 @@ def lower_to_target_ir(module: ModuleOp, tile_sizes: tuple[int, ...], halo_width
 def lower_fused_to_target_ir(modules: Sequence[ModuleOp], tile_sizes: tuple[int, ...],
                              halo_widths: tuple[int, ...], kernel_hints: dict | None = None,
                              spatial_term_order: bool | None = None, *, dtype: str | None = None,
-                             boundary_mode: str = "none") -> ModuleOp:
+                             boundary_mode: str = "none", kahan: bool = False) -> ModuleOp:
     meta = extract_fused_meta(modules, spatial_term_order, dtype=dtype)
+    if kahan:
+        apply_kahan(meta)
     kernel = _build_kernel_op(meta, tile_sizes, halo_widths, kernel_hints,
                               boundary_mode=boundary_mode)
     return ModuleOp([kernel, _build_host(meta, 1)])

@@ -59,7 +59,9 @@ def _internal_offsets(ndim: int, offsets) -> tuple[int, int, int]:
 def _parse_line(line: str):
     """``v3 = addf v1, a0 : f64`` -> ("v3", "addf", ["v1", "a0"], "f64", extra)."""
     if line.startswith("return "):
-        return ("", "return", [line.split()[1]], "", None)
+        parts = line.split()
+        idx = int(parts[2][1:]) if len(parts) > 2 else None
+        return ("", "return", [parts[1]], "", idx)
     lhs, rhs = line.split(" = ", 1)
     body, typ = rhs.rsplit(" : ", 1)
     parts = body.split(" ", 1)
@@ -98,11 +100,11 @@ class _BodyEmitter:
 
     def emit(self, lines: list[str], access_types: dict[str, str]) -> str:
         self.types.update(access_types)
-        result = None
+        self.returns = []
         for raw in lines:
             lhs, op, args, typ, extra = _parse_line(raw)
             if op == "return":
-                result = args[0]
+                self.returns.append((args[0], extra))
                 continue
             self.types[lhs] = typ
             if op == "const":
@@ -114,6 +116,8 @@ class _BodyEmitter:
             if op in ("addf", "subf", "mulf", "divf"):
                 fn = {"addf": "add", "subf": "sub", "mulf": "mul", "divf": "div"}[op]
                 expr = f"__{sfx}{fn}_rn({self.conv(args[0], tgt)}, {self.conv(args[1], tgt)})"
+            elif op == "cast":
+                expr = self.conv(args[0], tgt)
             elif op == "negf":
                 expr = f"-({self.conv(args[0], tgt)})"
             elif op == "absf":
@@ -139,7 +143,7 @@ class _BodyEmitter:
             else:
                 raise ValueError(f"unknown SSA op {op!r}")
             self.lines.append(f"const {ct} {self.name(lhs)} = {expr};")
-        return result
+        return self.returns
 
     def result_as(self, v: str, store_t: str) -> str:
         t = self.types[v]
@@ -186,10 +190,11 @@ def emit_body(kernel: KernelOp) -> str:
         access_types[f"a{j}"] = field_t
     for m, prog in enumerate(kernel.ssa_body.data):
         em = _BodyEmitter(f"p{m}_")
-        res = em.emit([s.data for s in prog], access_types)
+        rets = em.emit([s.data for s in prog], access_types)
         for line in em.lines:
             out.append("      " + line)
-        out.append(f"      o.v[{m}][k] = {em.result_as(res, store_t)};")
+        for res, idx in rets:
+            out.append(f"      o.v[{m if idx is None else idx}][k] = {em.result_as(res, store_t)};")
     out.append("    }")
     out.append("  }")
     out.append("};")
@@ -223,7 +228,8 @@ def engine_params(kernel: KernelOp) -> dict:
         (tx,) = tile
         rows, ty = 1, 1
     rz, ry, rx = _internal_radius(ndim, [a.data for a in kernel.radius.data])
-    nout = len(kernel.ssa_body.data)
+    nout = sum(max(1, sum(1 for s in prog if s.data.startswith("return")))
+               for prog in kernel.ssa_body.data)
     nin = len(kernel.input_names.data)
     return {
         "T": "float" if dtype in ("float32", "fp32") else "double",

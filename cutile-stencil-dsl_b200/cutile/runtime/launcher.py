@@ -243,6 +243,19 @@ def _input_names(ir) -> tuple:
     return tuple(_arg_names(f, b))
 
 
+def _precision(precision, dtype):
+    """(dtype, kahan) for a ``precision`` request."""
+    if precision is None:
+        return dtype, False
+    if precision == "fp64":
+        return "float64", False
+    if precision == "fp32":
+        return "float32", False
+    if precision == "fp32_kahan":
+        return "float32", True
+    raise ValueError(f"precision must be fp64, fp32 or fp32_kahan, got {precision!r}")
+
+
 def _plan_from(tile_sizes, kernel_hints, ndim, base_plan):
     from cutile.passes.tiling import EnginePlan
 
@@ -340,8 +353,14 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
             layout: str | None = None, brick_size: int = 32, align_halo: bool = True,
             occupancy: int | None = None, select: str | None = None, *,
             temporal_steps: int | None = None, tile_sizes: tuple[int, ...] | None = None,
-            kernel_hints: dict | None = None, dtype: str | None = None) -> CompileResult:
-    """Compile a ``@stencil`` function for the B200 engine (launcher.py:342-602)."""
+            kernel_hints: dict | None = None, dtype: str | None = None,
+            precision: str | None = None) -> CompileResult:
+    """Compile a ``@stencil`` function for the B200 engine (launcher.py:342-602).
+
+    ``precision`` (extension): ``"fp64"``, ``"fp32"`` or ``"fp32_kahan"`` --
+    the last stores fields in FP32 and applies the body, which must read
+    ``u + increment``, as a Kahan-compensated update with a compensation field
+    (``launch_<name>(u_in, c_in, u_out, c_out)``)."""
     from cutile.lowering.stencil_to_target import lower_to_target_ir
     from cutile.lowering.target_to_cuda import emit_cuda
     from cutile.passes.tiling import default_engine_plan, fit_plan
@@ -350,7 +369,7 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
         raise NotImplementedError("multi-GPU domain decomposition is not part of the B200 backend")
     ir = stencil_fn._ir
     name = stencil_fn._fn.__name__
-    dtype = dtype or getattr(stencil_fn, "_dtype", "float64")
+    dtype, kahan = _precision(precision, dtype or getattr(stencil_fn, "_dtype", "float64"))
     dtype_bytes = 4 if dtype in ("float32", "fp32") else 8
     if hw is not None:
         dtype_bytes = hw.dtype_bytes
@@ -377,6 +396,8 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
         if res.plan is not None:
             plan = res.plan
         T = res.temporal_steps
+    if kahan:
+        num_inputs += 1  # the compensation field
     if temporal_steps is not None:
         T = int(temporal_steps)
         if T > 1 and num_inputs != 1:
@@ -400,7 +421,8 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
         if "bc_type" in boundary_spec and "type" not in boundary_spec:
             boundary_spec["type"] = boundary_spec.pop("bc_type")
     target = lower_to_target_ir(ir.clone(), plan.tile_sizes(), halo_widths, temporal_steps=T,
-                                boundary_spec=boundary_spec, kernel_hints=hints, dtype=dtype)
+                                boundary_spec=boundary_spec, kernel_hints=hints, dtype=dtype,
+                                kahan=kahan)
     cuda = emit_cuda(target)
     kernels = {"main": name}
     if boundary_spec is not None:
@@ -408,27 +430,34 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
         bc_target = lower_to_target_ir(ir.clone(), bc_plan.tile_sizes(), halo_widths,
                                        temporal_steps=1, boundary_spec=boundary_spec,
                                        kernel_hints=bc_plan.hints(), dtype=dtype,
-                                       boundary_mode=boundary_spec.get("type", "dirichlet"))
+                                       boundary_mode=boundary_spec.get("type", "dirichlet"),
+                                       kahan=kahan)
         _rename_kernel(bc_target, f"{name}_bc")
         cuda += "\n" + emit_cuda(bc_target, preamble=False)
         kernels["fused_bc"] = f"{name}_bc"
     in_names = _input_names(ir)
-    multi = num_inputs > 1
+    n_fields = num_inputs - (1 if kahan else 0)
+    multi = n_fields > 1
+    names = ([n for n in "uvwxyz"][:n_fields] if n_fields <= 6 else
+             [f"arr{i}" for i in range(n_fields)]) if multi else ["u_in"]
+    outs = ["u_out"]
+    if kahan:
+        names = names + ["c_in"]
+        outs = ["u_out", "c_out"]
     spec = {
         "name": name, "ndim": len(stencil_halo), "dtype": dtype, "halo": list(halo_widths),
-        "stencil_halo": list(stencil_halo), "inputs": num_inputs, "outputs": 1,
+        "stencil_halo": list(stencil_halo), "inputs": num_inputs, "outputs": len(outs),
         "temporal_steps": T, "boundary": boundary_spec, "kernels": kernels,
-        "input_names": [n for n in "uvwxyz"][:num_inputs] if multi else ["u_in"],
-        "output_params": ["u_out"], "zchunk": plan.zchunk,
+        "input_names": names, "output_params": outs, "zchunk": plan.zchunk,
+        "precision": precision or ("fp32" if dtype == "float32" else "fp64"),
     }
-    if multi and num_inputs > 6:
-        spec["input_names"] = [f"arr{i}" for i in range(num_inputs)]
     code = generate_module_code(name, cuda, spec)
     return CompileResult(
         name=name, code=code, ndim=stencil_fn._ndim or len(halo_widths),
         halo_widths=tuple(halo_widths), tile_sizes=plan.tile_sizes(), temporal_steps=T,
         analysis=analysis, stencil_halo=tuple(stencil_halo), kernel_hints=hints,
-        resources=resources, inputs=in_names, cuda_source=cuda, dtype=dtype,
+        resources=resources, inputs=in_names + (("c_in",) if kahan else ()), cuda_source=cuda,
+        dtype=dtype,
         boundary=boundary_spec, layout=layout or "flat", brick_size=brick_size if layout == "bricked" else 0,
         _ref_fn=stencil_fn._fn, _ref_fns=[stencil_fn._fn])
 
@@ -452,7 +481,8 @@ def compile_fused(stencil_fns: list, domain: tuple[int, ...] | None = None, hw=N
                   halo_widths: tuple[int, ...] | None = None, temporal_steps: int = 1,
                   occupancy: int | None = None, align_halo: bool = True,
                   select: str | None = None, *, kernel_hints: dict | None = None,
-                  dtype: str | None = None, boundary=None) -> CompileResult:
+                  dtype: str | None = None, boundary=None,
+                  precision: str | None = None) -> CompileResult:
     """Several stencils over one domain in one multi-output kernel
     (launcher.py:610-728): each distinct (field, offset) is staged once and
     every output is stored.  ``boundary`` (extension) adds a ``step_<name>``
@@ -467,8 +497,12 @@ def compile_fused(stencil_fns: list, domain: tuple[int, ...] | None = None, hw=N
         raise NotImplementedError(
             "temporal blocking of fused kernels is not supported (temporal_steps must be 1)")
     modules = [fn._ir for fn in stencil_fns]
-    dtype = dtype or getattr(stencil_fns[0], "_dtype", "float64")
+    dtype, kahan = _precision(precision, dtype or getattr(stencil_fns[0], "_dtype", "float64"))
     meta = extract_fused_meta(modules, dtype=dtype)
+    if kahan:
+        from cutile.lowering.stencil_to_target import apply_kahan
+
+        apply_kahan(meta)
     ndim = meta.ndim
     dtype_bytes = 4 if dtype in ("float32", "fp32") else 8
     if hw is not None:
@@ -492,7 +526,7 @@ def compile_fused(stencil_fns: list, domain: tuple[int, ...] | None = None, hw=N
     if occupancy is not None:
         hints["occupancy"] = occupancy
     target = lower_fused_to_target_ir(modules, plan.tile_sizes(), tuple(halo_widths), hints,
-                                      dtype=dtype)
+                                      dtype=dtype, kahan=kahan)
     cuda = emit_cuda(target)
     kernels = {"main": meta.name}
     bspec = None
@@ -500,7 +534,8 @@ def compile_fused(stencil_fns: list, domain: tuple[int, ...] | None = None, hw=N
         bspec = {"type": boundary} if isinstance(boundary, str) else (
             dict(boundary) if isinstance(boundary, dict) else boundary.to_dict())
         bc_target = lower_fused_to_target_ir(modules, plan.tile_sizes(), tuple(halo_widths), hints,
-                                             dtype=dtype, boundary_mode=bspec["type"])
+                                             dtype=dtype, boundary_mode=bspec["type"],
+                                             kahan=kahan)
         _rename_kernel(bc_target, f"{meta.name}_bc")
         cuda += "\n" + emit_cuda(bc_target, preamble=False)
         kernels["fused_bc"] = f"{meta.name}_bc"
@@ -509,14 +544,16 @@ def compile_fused(stencil_fns: list, domain: tuple[int, ...] | None = None, hw=N
         "stencil_halo": list(stencil_halo), "inputs": meta.num_inputs,
         "outputs": meta.num_outputs, "temporal_steps": 1, "boundary": bspec, "kernels": kernels,
         "input_names": list(meta.input_names), "output_params": meta.output_params(),
-        "zchunk": plan.zchunk,
+        "zchunk": plan.zchunk, "precision": precision or ("fp32" if dtype == "float32" else "fp64"),
     }
     code = generate_module_code(meta.name, cuda, spec)
     return CompileResult(
         name=meta.name, code=code, ndim=ndim, halo_widths=tuple(halo_widths),
         tile_sizes=plan.tile_sizes(), temporal_steps=1, analysis={"unique_loads": num_loads},
         stencil_halo=stencil_halo, kernel_hints=hints, resources=None,
-        inputs=tuple(meta.input_names), outputs=tuple(meta.output_names), cuda_source=cuda,
+        inputs=tuple(meta.input_names),
+        outputs=tuple(meta.output_names) + (tuple(f"{n}_c" for n in meta.output_names) if kahan
+                                            else ()), cuda_source=cuda,
         dtype=dtype, boundary=bspec, _ref_fns=[fn._fn for fn in stencil_fns],
         _ref_inputs=meta.stencil_inputs)
 

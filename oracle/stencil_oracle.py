@@ -296,3 +296,43 @@ def temporal_depth(tile, halo, max_steps: int = 8, smem: int = 49152, dtype_byte
 
 
 __all__ = [name for name in dir() if not name.startswith("_")]
+
+
+def kahan_update(u_in, c_in, incr):
+    """Kahan-compensated ``u += incr`` in the arrays' dtype (float32):
+    ``y = incr - c; t = u + y; c' = (t - u) - y``; returns ``(t, c')``."""
+    dt = u_in.dtype
+    y = np.asarray(incr, dtype=dt) - c_in
+    t = u_in + y
+    c2 = (t - u_in) - y
+    return t, c2
+
+
+def fused_kahan_step(inputs_by_name: dict, comps: dict, incr_fns: dict, ndim: int, halo,
+                     boundary: str | None = None):
+    """One step of a Kahan-compensated fused update.
+
+    ``incr_fns`` maps an updated field name to its increment function;
+    ``comps`` maps the field name to its compensation array.  With a
+    boundary kind, the inputs are boundary-filled (copies) first, as the
+    fused-boundary kernels stage them.  Returns ``{name: (u_new, c_new)}``
+    with only the interiors meaningful.
+    """
+    ins = {}
+    for k, a in inputs_by_name.items():
+        b = a.copy()
+        if boundary is not None:
+            apply_boundary(b, uniform_spec(boundary, ndim), halo)
+        ins[k] = b
+    first = next(iter(ins.values()))
+    inner = _interior(first.shape, halo)
+    out = {}
+    for name, fn in incr_fns.items():
+        incr = evaluate(ins, fn, ndim, halo, first.shape, first.dtype)
+        t, c2 = kahan_update(ins[name][inner], comps[name][inner], incr)
+        u_new = np.zeros_like(first)
+        c_new = np.zeros_like(first)
+        u_new[inner] = t
+        c_new[inner] = c2
+        out[name] = (u_new, c_new)
+    return out

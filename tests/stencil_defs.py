@@ -113,3 +113,32 @@ CASES = {
     "update_e": (update_e, 1, 2), "cond3d": (cond3d, 3, 1), "clip1d": (clip1d, 1, 1),
     "box27": (box27, 3, 1),
 }
+
+
+# Increments of the Gray-Scott updates (gs_u = u + gs_u_incr, gs_v = v + gs_v_incr);
+# the Kahan-compensated FP32 mode adds the increment with compensation.
+def gs_u_incr(u, v, i, j):
+    return DT_GS * (DU * (u[i - 1, j] + u[i + 1, j] + u[i, j - 1] + u[i, j + 1] - 4 * u[i, j])
+                    - u[i, j] * v[i, j] * v[i, j] + F_GS * (1.0 - u[i, j]))
+
+
+def gs_v_incr(u, v, i, j):
+    return DT_GS * (DV * (v[i - 1, j] + v[i + 1, j] + v[i, j - 1] + v[i, j + 1] - 4 * v[i, j])
+                    + u[i, j] * v[i, j] * v[i, j] - (F_GS + K_GS) * v[i, j])
+
+
+def gray_scott_init(n: int, seed: int = 2, halo=(1, 1), dtype="float64"):
+    """4096^2-style Gray-Scott start: u=1, v=0, then 20 random 32x32 squares set
+    to u=0.5, v=0.25 with +-1% uniform noise (seeded)."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    shape = (n + 2 * halo[0], n + 2 * halo[1])
+    u = np.ones(shape)
+    v = np.zeros(shape)
+    for _ in range(20):
+        y, x = rng.integers(0, n - 32, size=2)
+        sl = (slice(halo[0] + y, halo[0] + y + 32), slice(halo[1] + x, halo[1] + x + 32))
+        u[sl] = 0.5 * (1 + rng.uniform(-0.01, 0.01, (32, 32)))
+        v[sl] = 0.25 * (1 + rng.uniform(-0.01, 0.01, (32, 32)))
+    return u.astype(dtype), v.astype(dtype)
