@@ -296,3 +296,30 @@ extern "C" int csd_reduce_noalloc(const csd_field* a, const csd_field* b, const 
   if (rc) return rc;
   return csd_reduce(a, b, halo, op, partials, nblocks, result, stream);
 }
+
+// ---------------------------------------------------------------------------
+// CFL time-step control for batched solvers: dt[i] = cfl * scale[i] / smax[i]
+// (smax = the per-grid maximum signal speed from a max-reduction launch),
+// then smax[i] = 0 so the next reduction starts afresh.  One thread per grid.
+// ---------------------------------------------------------------------------
+namespace {
+__global__ void cfl_update_kernel(int n, double* smax, const double* scale, double cfl,
+                                  double dt_max, double* dt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double s = smax[i];
+  double v = (s > 0.0) ? __ddiv_rn(__dmul_rn(cfl, scale[i]), s) : dt_max;
+  if (v > dt_max) v = dt_max;
+  dt[i] = v;
+  smax[i] = 0.0;
+}
+}  // namespace
+
+extern "C" int csd_cfl_update(int n, double* smax, const double* scale, double cfl, double dt_max,
+                              double* dt, void* stream) {
+  if (n < 1 || !smax || !scale || !dt) return csd_internal_fail(CSD_EINVAL, "bad cfl arguments");
+  cfl_update_kernel<<<(n + 127) / 128, 128, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+      n, smax, scale, cfl, dt_max, dt);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? CSD_OK : csd_internal_fail(CSD_ELAUNCH, cudaGetErrorString(e));
+}

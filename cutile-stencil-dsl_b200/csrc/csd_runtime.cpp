@@ -323,7 +323,9 @@ extern "C" {
 
 int csd_internal_fail(int code, const char* msg) { return fail(code, "%s", msg); }
 
-int csd_version(void) { return 100; }
+int csd_version(void) { return 101; }
+
+size_t csd_grid_size(void) { return sizeof(csd_grid); }
 
 const char* csd_last_error(void) { return g_last_error.c_str(); }
 
@@ -466,10 +468,15 @@ static bool contiguous(const csd_field& f) {
   return true;
 }
 
-int csd_launch(csd_kernel* k, const csd_field* in, int n_in, const csd_field* out, int n_out,
-               const csd_launch_opts* opts, void* stream) {
-  if (!k || !in || !out) return fail(CSD_EINVAL, "null argument");
+// Validate one grid's fields and fill its kernel-side descriptor.
+static int build_grid(csd_kernel* k, const csd_field* in, int n_in, const csd_field* out,
+                      int n_out, const csd_launch_opts& o, DeviceState* st, int loader_req,
+                      csd_grid* g, int* loader_out) {
   const csd_kernel_desc& D = k->desc;
+  if (!in || (!out && n_out > 0)) return fail(CSD_EINVAL, "null field array");
+  if (D.reduce_max && !o.red)
+    return fail(CSD_EINVAL, "kernel %s max-reduces: opts.red must point to a device double",
+                k->name.c_str());
   if (n_in != D.nin || n_out != D.nout)
     return fail(CSD_EINVAL, "kernel %s takes %d inputs and %d outputs, got %d and %d",
                 k->name.c_str(), D.nin, D.nout, n_in, n_out);
@@ -488,7 +495,95 @@ int csd_launch(csd_kernel* k, const csd_field* in, int n_in, const csd_field* ou
     if ((reinterpret_cast<uintptr_t>(f.ptr) % D.dtype_bytes) != 0)
       return fail(CSD_EALIGN, "field pointer not aligned to its element size");
   }
-  csd_launch_opts o = {};
+  if (D.ndyn > 0 && !o.dyn) return fail(CSD_EINVAL, "kernel %s reads device scalars: opts.dyn is null",
+                                        k->name.c_str());
+  memset(g, 0, sizeof(*g));
+  int halo[3];
+  view3(f0, g->dims, o.halo, halo);
+  g->ndim = f0.ndim;
+  // per-step radius: chained steps see zero halos beyond the interior, so the
+  // array needs only one step's halo
+  const int rad[3] = {D.rz / D.temporal, D.ry / D.temporal, D.rx / D.temporal};
+  for (int d = 0; d < 3; ++d) {
+    g->halo[d] = halo[d];
+    g->interior[d] = (int)(g->dims[d] - 2 * halo[d]);
+    if (g->interior[d] <= 0 && g->dims[d] > 0)
+      return fail(CSD_EINVAL, "array extent %lld leaves no interior with halo %d", g->dims[d], halo[d]);
+    if (halo[d] < rad[d])
+      return fail(CSD_EINVAL, "array halo %d is smaller than the stencil radius %d", halo[d], rad[d]);
+  }
+  g->pitch_y = g->dims[2];
+  g->pitch_z = g->dims[1] * g->dims[2];
+  for (int i = 0; i < n_in; ++i) g->in[i] = in[i].ptr;
+  for (int i = 0; i < n_out; ++i) g->out[i] = out[i].ptr;
+  g->xbase = (g->halo[2] / D.align) * D.align;
+  g->tiles[0] = (g->halo[2] + g->interior[2] - g->xbase + D.tile_x - 1) / D.tile_x;
+  g->tiles[1] = (g->interior[1] + D.tile_y - 1) / D.tile_y;
+  const long long esz = D.dtype_bytes;
+  // Loader: TMA when every input is 16-byte aligned with 16-byte pitches.
+  bool tma_ok = ((g->dims[2] * esz) % 16 == 0) && ((g->pitch_z * esz) % 16 == 0);
+  for (int i = 0; i < n_in; ++i) tma_ok = tma_ok && (reinterpret_cast<uintptr_t>(in[i].ptr) % 16 == 0);
+  int loader = loader_req;
+  if (loader < 0 || loader > 1) loader = tma_ok ? CSD_LOADER_TMA : CSD_LOADER_LDG;
+  if (loader == CSD_LOADER_TMA && !tma_ok)
+    return fail(CSD_EALIGN, "TMA path needs 16-byte aligned fields and row pitch");
+  // Work items (column tiles x Z chunks) sized so that they fill the
+  // resident CTAs in one wave: items of equal length that start together
+  // keep neighbouring columns on the same planes (their halo rows are then
+  // shared in L2) and leave no tail.
+  const long long slots = o.grid > 0 ? o.grid : (long long)k->blocks_per_sm[loader] * st->sms;
+  const long long columns = (long long)g->tiles[0] * g->tiles[1];
+  int zchunk = o.zchunk > 0 ? o.zchunk : D.zchunk;
+  if (zchunk <= 0) {
+    long long nzc = slots / (columns > 0 ? columns : 1);
+    if (nzc < 1) nzc = 1;
+    if (nzc > g->interior[0]) nzc = g->interior[0];
+    zchunk = (int)((g->interior[0] + nzc - 1) / nzc);
+  }
+  g->zchunk = ((zchunk + D.rows - 1) / D.rows) * D.rows;
+  if (g->zchunk > g->interior[0]) g->zchunk = ((g->interior[0] + D.rows - 1) / D.rows) * D.rows;
+  g->tiles[2] = (g->interior[0] + g->zchunk - 1) / g->zchunk;
+  long long items = columns * g->tiles[2];
+  if (items > 0x7fffffff) return fail(CSD_EINVAL, "too many work items");
+  g->items = (int)items;
+  g->bc_value = o.bc_value;
+  for (int i = 0; i < CSD_MAX_SCALARS; ++i) g->scalars[i] = o.scalars[i];
+  for (int i = 0; i < CSD_MAX_FIELDS; ++i) g->bc_odd[i] = o.bc_odd[i];
+  g->dyn = o.dyn;
+  g->red = o.red;
+  bool vec = true;
+  for (int i = 0; i < n_out; ++i) vec = vec && (reinterpret_cast<uintptr_t>(out[i].ptr) % 16 == 0);
+  vec = vec && ((g->pitch_y * esz) % 16 == 0) && ((g->pitch_z * esz) % 16 == 0);
+  g->vec_store = vec ? 1 : 0;
+  if (loader == CSD_LOADER_TMA) {
+    Driver& d = drv();
+    for (int i = 0; i < n_in; ++i) {
+      unsigned long long gdim[3] = {(unsigned long long)g->dims[2], (unsigned long long)g->dims[1],
+                                    (unsigned long long)g->dims[0]};
+      unsigned long long gstride[2] = {(unsigned long long)(g->pitch_y * esz),
+                                       (unsigned long long)(g->pitch_z * esz)};
+      unsigned box[3] = {(unsigned)D.box_w, (unsigned)D.box_h, (unsigned)D.rows};
+      unsigned estride[3] = {1, 1, 1};
+      CUresult r = d.cuTensorMapEncodeTiled(&g->tmap[i], esz == 8 ? TMAP_FLOAT64 : TMAP_FLOAT32, 3,
+                                            in[i].ptr, gdim, gstride, box, estride,
+                                            0 /*interleave none*/, 0 /*swizzle none*/,
+                                            2 /*L2 promotion 128B*/, 0 /*OOB fill zeros*/);
+      if (r) return cu_fail(r, "cuTensorMapEncodeTiled");
+    }
+  }
+  *loader_out = loader;
+  return CSD_OK;
+}
+
+int csd_launch(csd_kernel* k, const csd_field* in, int n_in, const csd_field* out, int n_out,
+               const csd_launch_opts* opts, void* stream) {
+  if (!k) return fail(CSD_EINVAL, "null kernel");
+  if (k->desc.reduce_max && !(opts && opts->red))
+    return fail(CSD_EINVAL, "kernel %s max-reduces: opts.red must point to a device double",
+                k->name.c_str());
+  csd_launch_opts o;
+  memset(&o, 0, sizeof(o));
+  o.loader = -1;
   if (opts) o = *opts;
   CUdevice dev;
   int rc = ensure_context(&dev);
@@ -496,90 +591,72 @@ int csd_launch(csd_kernel* k, const csd_field* in, int n_in, const csd_field* ou
   DeviceState* st;
   rc = device_state(dev, &st);
   if (rc) return rc;
-
   csd_params p;
   memset(&p, 0, sizeof(p));
-  int halo[3];
-  view3(f0, p.dims, o.halo, halo);
-  // per-step radius: chained steps see zero halos beyond the interior, so the
-  // array needs only one step's halo
-  const int rad[3] = {D.rz / D.temporal, D.ry / D.temporal, D.rx / D.temporal};
-  for (int d = 0; d < 3; ++d) {
-    p.halo[d] = halo[d];
-    p.interior[d] = (int)(p.dims[d] - 2 * halo[d]);
-    if (p.interior[d] <= 0 && p.dims[d] > 0)
-      return fail(CSD_EINVAL, "array extent %lld leaves no interior with halo %d", p.dims[d], halo[d]);
-    if (halo[d] < rad[d])
-      return fail(CSD_EINVAL, "array halo %d is smaller than the stencil radius %d", halo[d], rad[d]);
-  }
-  p.pitch_y = p.dims[2];
-  p.pitch_z = p.dims[1] * p.dims[2];
-  for (int i = 0; i < n_in; ++i) p.in[i] = in[i].ptr;
-  for (int i = 0; i < n_out; ++i) p.out[i] = out[i].ptr;
-  p.xbase = (p.halo[2] / D.align) * D.align;
-  p.tiles[0] = (p.halo[2] + p.interior[2] - p.xbase + D.tile_x - 1) / D.tile_x;
-  p.tiles[1] = (p.interior[1] + D.tile_y - 1) / D.tile_y;
-  // Persistent CTAs that fit at once; the work items (column tiles x Z
-  // chunks) are sized so that they fill these slots in one wave: items of
-  // equal length that start together keep neighbouring columns on the same
-  // planes (their halo rows are then shared in L2) and leave no tail.
-  int loader_guess = o.loader == CSD_LOADER_LDG ? CSD_LOADER_LDG : CSD_LOADER_TMA;
-  const long long slots = o.grid > 0 ? o.grid : (long long)k->blocks_per_sm[loader_guess] * st->sms;
-  const long long columns = (long long)p.tiles[0] * p.tiles[1];
-  int zchunk = o.zchunk > 0 ? o.zchunk : D.zchunk;
-  if (zchunk <= 0) {
-    long long nzc = slots / (columns > 0 ? columns : 1);
-    if (nzc < 1) nzc = 1;
-    if (nzc > p.interior[0]) nzc = p.interior[0];
-    zchunk = (int)((p.interior[0] + nzc - 1) / nzc);
-  }
-  p.zchunk = ((zchunk + D.rows - 1) / D.rows) * D.rows;
-  if (p.zchunk > p.interior[0]) p.zchunk = ((p.interior[0] + D.rows - 1) / D.rows) * D.rows;
-  p.tiles[2] = (p.interior[0] + p.zchunk - 1) / p.zchunk;
-  long long items = (long long)p.tiles[0] * p.tiles[1] * p.tiles[2];
-  if (items > 0x7fffffff) return fail(CSD_EINVAL, "too many work items");
-  p.items = (int)items;
-  p.bc_mode = D.bc_mode;
-  p.bc_value = o.bc_value;
+  int loader = 0;
+  rc = build_grid(k, in, n_in, out, n_out, o, st, o.loader, &p.g, &loader);
+  if (rc) return rc;
   p.err = reinterpret_cast<int*>(st->err);
   p.timeout_ns = o.timeout_ns ? o.timeout_ns : 2000000000ull;
-  const long long esz = D.dtype_bytes;
-  bool vec = true;
-  for (int i = 0; i < n_out; ++i) vec = vec && (reinterpret_cast<uintptr_t>(out[i].ptr) % 16 == 0);
-  vec = vec && ((p.pitch_y * esz) % 16 == 0) && ((p.pitch_z * esz) % 16 == 0);
-  p.vec_store = vec ? 1 : 0;
-
-  // Loader: TMA when every input is 16-byte aligned with 16-byte pitches.
-  bool tma_ok = ((p.dims[2] * esz) % 16 == 0) && ((p.pitch_z * esz) % 16 == 0);
-  for (int i = 0; i < n_in; ++i) tma_ok = tma_ok && (reinterpret_cast<uintptr_t>(in[i].ptr) % 16 == 0);
-  int loader = o.loader;
-  if (loader < 0 || loader > 1) loader = tma_ok ? CSD_LOADER_TMA : CSD_LOADER_LDG;
-  if (loader == CSD_LOADER_TMA && !tma_ok)
-    return fail(CSD_EALIGN, "TMA path needs 16-byte aligned fields and row pitch");
-  if (loader == CSD_LOADER_TMA) {
-    Driver& d = drv();
-    for (int i = 0; i < n_in; ++i) {
-      unsigned long long gdim[3] = {(unsigned long long)p.dims[2], (unsigned long long)p.dims[1],
-                                    (unsigned long long)p.dims[0]};
-      unsigned long long gstride[2] = {(unsigned long long)(p.pitch_y * esz),
-                                       (unsigned long long)(p.pitch_z * esz)};
-      unsigned box[3] = {(unsigned)D.box_w, (unsigned)D.box_h, (unsigned)D.rows};
-      unsigned estride[3] = {1, 1, 1};
-      CUresult r = d.cuTensorMapEncodeTiled(&p.tmap[i], esz == 8 ? TMAP_FLOAT64 : TMAP_FLOAT32, 3,
-                                            in[i].ptr, gdim, gstride, box, estride,
-                                            0 /*interleave none*/, 0 /*swizzle none*/,
-                                            2 /*L2 promotion 128B*/, 0 /*OOB fill zeros*/);
-      if (r) return cu_fail(r, "cuTensorMapEncodeTiled");
-    }
-  }
   int grid = o.grid > 0 ? o.grid : k->blocks_per_sm[loader] * st->sms;
-  if (grid > p.items) grid = p.items;
+  if (grid > p.g.items) grid = p.g.items;
   if (grid < 1) return CSD_OK;  // nothing to do
   void* args[] = {&p};
-  CUresult r = drv().cuLaunchKernel(k->fn[loader], (unsigned)grid, 1, 1, (unsigned)D.threads, 1, 1,
-                                    (unsigned)D.smem_bytes, reinterpret_cast<CUstream>(stream), args,
-                                    nullptr);
+  CUresult r = drv().cuLaunchKernel(k->fn[loader], (unsigned)grid, 1, 1, (unsigned)k->desc.threads,
+                                    1, 1, (unsigned)k->desc.smem_bytes,
+                                    reinterpret_cast<CUstream>(stream), args, nullptr);
   if (r) return cu_fail(r, "cuLaunchKernel");
+  return CSD_OK;
+}
+
+int csd_grid_build(csd_kernel* k, const csd_field* in, int n_in, const csd_field* out, int n_out,
+                   const csd_launch_opts* opts, csd_grid* g, int* items, int* loader_used) {
+  if (!k || !g) return fail(CSD_EINVAL, "null argument");
+  csd_launch_opts o;
+  memset(&o, 0, sizeof(o));
+  if (opts) o = *opts;
+  CUdevice dev;
+  int rc = ensure_context(&dev);
+  if (rc) return rc;
+  DeviceState* st;
+  rc = device_state(dev, &st);
+  if (rc) return rc;
+  int loader = 0;
+  rc = build_grid(k, in, n_in, out, n_out, o, st, o.loader, g, &loader);
+  if (rc) return rc;
+  if (items) *items = g->items;
+  if (loader_used) *loader_used = loader;
+  return CSD_OK;
+}
+
+int csd_launch_batch(csd_kernel* k, const csd_grid* grids, const int* item_start, int ngrids,
+                     int total_items, const csd_launch_opts* opts, void* stream) {
+  if (!k || !grids || !item_start || ngrids < 1) return fail(CSD_EINVAL, "bad batch arguments");
+  if (total_items < 1) return CSD_OK;
+  if ((reinterpret_cast<uintptr_t>(grids) % 64) != 0)
+    return fail(CSD_EALIGN, "grid descriptors must be 64-byte aligned in device memory");
+  CUdevice dev;
+  int rc = ensure_context(&dev);
+  if (rc) return rc;
+  DeviceState* st;
+  rc = device_state(dev, &st);
+  if (rc) return rc;
+  csd_params p;
+  memset(&p, 0, sizeof(p));
+  p.grids = grids;
+  p.item_start = item_start;
+  p.ngrids = ngrids;
+  p.total_items = total_items;
+  p.err = reinterpret_cast<int*>(st->err);
+  p.timeout_ns = (opts && opts->timeout_ns) ? opts->timeout_ns : 2000000000ull;
+  const int loader = (opts && opts->loader == CSD_LOADER_LDG) ? CSD_LOADER_LDG : CSD_LOADER_TMA;
+  int grid = (opts && opts->grid > 0) ? opts->grid : k->blocks_per_sm[loader] * st->sms;
+  if (grid > total_items) grid = total_items;
+  void* args[] = {&p};
+  CUresult r = drv().cuLaunchKernel(k->fn[loader], (unsigned)grid, 1, 1,
+                                    (unsigned)k->desc.threads, 1, 1, (unsigned)k->desc.smem_bytes,
+                                    reinterpret_cast<CUstream>(stream), args, nullptr);
+  if (r) return cu_fail(r, "cuLaunchKernel(batch)");
   return CSD_OK;
 }
 

@@ -51,7 +51,7 @@ __host__ __device__ constexpr int imax(int a, int b) { return a > b ? a : b; }
 // Compile-time configuration
 // ---------------------------------------------------------------------------
 template <typename T_, int NIN_, int NOUT_, int RZ_, int RY_, int RX_, int ROWS_, int TY_, int TX_,
-          int NT_, int STAGES_, int TEMPORAL_, int LOADER_, int BC_>
+          int NT_, int STAGES_, int TEMPORAL_, int LOADER_, int BC_, int REDUCE_ = 0>
 struct Cfg {
   typedef T_ T;
   static constexpr int NIN = NIN_, NOUT = NOUT_;
@@ -59,6 +59,7 @@ struct Cfg {
   static constexpr int ROWS = ROWS_, TY = TY_, TX = TX_;
   static constexpr int NT = NT_, STAGES = STAGES_, TEMPORAL = TEMPORAL_;
   static constexpr int LOADER = LOADER_, BC = BC_;
+  static constexpr int REDUCE = REDUCE_;  // 1: max-reduce output 0 into grid.red, store nothing
   static constexpr int ALIGN = 16 / (int)sizeof(T);
   static constexpr int VEC = ALIGN;
   static constexpr int HC = RZ > 0 ? cdiv(RZ, ROWS) : 0;  // halo chunks per side, per step
@@ -130,6 +131,11 @@ struct TileView {
   int slot_elems;
   int height;             // Y rows per chunk row
   int y_off;              // buffer row of the unit's y (source has extra halo rows)
+  const double* scal;     // per-grid constants (csd_grid.scalars)
+  const double* dyn;      // per-grid device scalars (csd_grid.dyn)
+
+  __device__ __forceinline__ double scalar(int k) const { return scal[k]; }
+  __device__ __forceinline__ double dynamic(int k) const { return dyn[k]; }
 
   // Row segment of field F at Z offset DZ and Y offset DY for unit (r, y, x).
   template <int F, int DZ, int DY, int LO, int HI>
@@ -180,21 +186,21 @@ template <class C>
 struct Loader {
   typedef typename C::T T;
 
-  // Issue the copies of one chunk (all fields) into `slot`.
-  static __device__ __forceinline__ void issue(const csd_params& p, T* ring, unsigned bar,
-                                               int slot, int x0, int y0, int z0) {
+  // Issue the copies of one chunk (all fields) of grid `g` into `slot`.
+  static __device__ __forceinline__ void issue(const csd_grid& g, T* ring, unsigned bar, int slot,
+                                               int x0, int y0, int z0) {
     if constexpr (C::LOADER == CSD_LOADER_TMA) {
       if (threadIdx.x == 0) {
         ptx::mbar_arrive_expect_tx(bar, (unsigned)(C::CHUNK_BYTES * C::NIN));
 #pragma unroll
         for (int f = 0; f < C::NIN; ++f) {
           T* dst = ring + (f * C::NSLOT + slot) * C::SLOT_ELEMS;
-          ptx::tma_load_3d(ptx::smem_addr(dst), &p.tmap[f], x0, y0, z0, bar);
+          ptx::tma_load_3d(ptx::smem_addr(dst), &g.tmap[f], x0, y0, z0, bar);
         }
       }
     } else {
       constexpr int N = C::ROWS * C::BOXH * C::BOXW;
-      const long long NZ = p.dims[0], NY = p.dims[1], NX = p.dims[2];
+      const long long NZ = g.dims[0], NY = g.dims[1], NX = g.dims[2];
 #pragma unroll 1
       for (int e = threadIdx.x; e < N; e += C::NT) {
         const int xx = e % C::BOXW;
@@ -203,11 +209,11 @@ struct Loader {
         const int rr = t / C::BOXH;
         const long long gx = (long long)x0 + xx, gy = (long long)y0 + yy, gz = (long long)z0 + rr;
         const bool ok = gx >= 0 && gx < NX && gy >= 0 && gy < NY && gz >= 0 && gz < NZ;
-        const long long off = ok ? (gz * p.pitch_z + gy * p.pitch_y + gx) : 0;
+        const long long off = ok ? (gz * g.pitch_z + gy * g.pitch_y + gx) : 0;
 #pragma unroll
         for (int f = 0; f < C::NIN; ++f) {
           T* dst = ring + (f * C::NSLOT + slot) * C::SLOT_ELEMS + e;
-          const T* src = reinterpret_cast<const T*>(p.in[f]) + off;
+          const T* src = reinterpret_cast<const T*>(g.in[f]) + off;
           ptx::cp_async_zfill<sizeof(T)>(ptx::smem_addr(dst), src, ok);
         }
       }
@@ -218,12 +224,14 @@ struct Loader {
 
 // Overwrite the cells of a freshly landed chunk that lie outside the domain
 // interior with their boundary-condition values (fused boundary fill).
+// `bc_odd[f]` bit d: a value mirrored across a boundary of dim d changes
+// sign (a wall's normal momentum); the sign is the product over mirrored dims.
 template <class C>
-__device__ __forceinline__ void patch_boundary(const csd_params& p, typename C::T* ring, int slot,
+__device__ __forceinline__ void patch_boundary(const csd_grid& g, typename C::T* ring, int slot,
                                                int x0, int y0, int z0) {
   typedef typename C::T T;
-  const int hz = p.halo[0], hy = p.halo[1], hx = p.halo[2];
-  const int nz = p.interior[0], ny = p.interior[1], nx = p.interior[2];
+  const int hz = g.halo[0], hy = g.halo[1], hx = g.halo[2];
+  const int nz = g.interior[0], ny = g.interior[1], nx = g.interior[2];
   const bool edge = x0 < hx || x0 + C::BOXW > hx + nx || y0 < hy || y0 + C::BOXH > hy + ny ||
                     z0 < hz || z0 + C::ROWS > hz + nz;
   if (!edge) return;
@@ -238,24 +246,60 @@ __device__ __forceinline__ void patch_boundary(const csd_params& p, typename C::
                         gz < hz + nz;
     if (inside) continue;
     // cells beyond the array's own extent are never read by interior points
-    if (gx < 0 || gy < 0 || gz < 0 || gx >= p.dims[2] || gy >= p.dims[1] || gz >= p.dims[0])
+    if (gx < 0 || gy < 0 || gz < 0 || gx >= g.dims[2] || gy >= g.dims[1] || gz >= g.dims[0])
       continue;
+    const bool out_x = (gx < hx || gx >= hx + nx) && g.dims[2] > 1;
+    const bool out_y = (gy < hy || gy >= hy + ny) && g.dims[1] > 1;
+    const bool out_z = (gz < hz || gz >= hz + nz) && g.dims[0] > 1;
 #pragma unroll
     for (int f = 0; f < C::NIN; ++f) {
       T v;
       if (C::BC == CSD_BC_DIRICHLET) {
-        v = (T)p.bc_value;
+        v = (T)g.bc_value;
       } else {
-        const long long mx = (nx > 0 && p.dims[2] > 1) ? bc_map(gx, hx, nx, C::BC) : gx;
-        const long long my = (ny > 0 && p.dims[1] > 1) ? bc_map(gy, hy, ny, C::BC) : gy;
-        const long long mz = (nz > 0 && p.dims[0] > 1) ? bc_map(gz, hz, nz, C::BC) : gz;
-        v = reinterpret_cast<const T*>(p.in[f])[mz * p.pitch_z + my * p.pitch_y + mx];
+        const long long mx = out_x ? bc_map(gx, hx, nx, C::BC) : gx;
+        const long long my = out_y ? bc_map(gy, hy, ny, C::BC) : gy;
+        const long long mz = out_z ? bc_map(gz, hz, nz, C::BC) : gz;
+        v = reinterpret_cast<const T*>(g.in[f])[mz * g.pitch_z + my * g.pitch_y + mx];
+        if (C::BC == CSD_BC_REFLECTING) {
+          // internal dims (Z, Y, X) <- array dims; bc_odd uses array dim numbers
+          const int odd = g.bc_odd[f];
+          const int nd = g.ndim;
+          bool flip = false;
+          if (nd == 3) flip = ((odd & 1) && out_z) ^ ((odd & 2) && out_y) ^ ((odd & 4) && out_x);
+          else if (nd == 2) flip = ((odd & 1) && out_z) ^ ((odd & 2) && out_x);
+          else flip = (odd & 1) && out_x;
+          if (flip) v = -v;
+        }
       }
       ring[(f * C::NSLOT + slot) * C::SLOT_ELEMS + e] = v;
     }
   }
   // the slot will be refilled by TMA (async proxy) after these generic writes
   ptx::fence_proxy_async_smem();
+}
+
+__device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
+  // non-negative doubles order like their bit patterns (NaN above +inf)
+  atomicMax(reinterpret_cast<unsigned long long*>(addr),
+            (unsigned long long)__double_as_longlong(v));
+}
+
+// Grid and local item of global work item `item` (batched: binary search of
+// the items prefix; single grid: the inline descriptor).
+__device__ __forceinline__ const csd_grid& grid_of(const csd_params& p, int item, int& local) {
+  if (p.grids == nullptr) {
+    local = item;
+    return p.g;
+  }
+  int lo = 0, hi = p.ngrids - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (p.item_start[mid] <= item) lo = mid;
+    else hi = mid - 1;
+  }
+  local = item - p.item_start[lo];
+  return p.grids[lo];
 }
 
 // ---------------------------------------------------------------------------
@@ -271,6 +315,7 @@ __device__ __forceinline__ void stream_engine(const csd_params& p) {
   T* inter = ring + C::RING_ELEMS;
   unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem_raw + C::BAR_OFFSET);
   __shared__ int abort_flag;
+  __shared__ double red_warp[32];
 
   if (threadIdx.x == 0) {
     abort_flag = 0;
@@ -285,44 +330,48 @@ __device__ __forceinline__ void stream_engine(const csd_params& p) {
   for (int e = threadIdx.x; e < C::INTER_ELEMS; e += C::NT) inter[e] = T(0);
   __syncthreads();
 
-  const int hz = p.halo[0], hy = p.halo[1], hx = p.halo[2];
-  const int nz = p.interior[0], ny = p.interior[1], nx = p.interior[2];
   constexpr int T_ = C::TEMPORAL;
   constexpr int HCT = C::HC * T_;  // input halo chunks per side for the whole chain
   unsigned seq = 0;                // chunks consumed by this CTA so far
+  const int total = p.grids == nullptr ? p.g.items : p.total_items;
 
-  for (int item = blockIdx.x; item < p.items; item += gridDim.x) {
-    const int tx = item % p.tiles[0];
-    const int t1 = item / p.tiles[0];
-    const int ty = t1 % p.tiles[1];
-    const int tz = t1 / p.tiles[1];
-    const int X0 = p.xbase + tx * C::TX;  // array column of the tile's first point
+  for (int gitem = blockIdx.x; gitem < total; gitem += gridDim.x) {
+    int item;
+    const csd_grid& g = grid_of(p, gitem, item);
+    const int hz = g.halo[0], hy = g.halo[1], hx = g.halo[2];
+    const int nz = g.interior[0], ny = g.interior[1], nx = g.interior[2];
+    const int tx = item % g.tiles[0];
+    const int t1 = item / g.tiles[0];
+    const int ty = t1 % g.tiles[1];
+    const int tz = t1 / g.tiles[1];
+    const int X0 = g.xbase + tx * C::TX;  // array column of the tile's first point
     const int Y0 = hy + ty * C::TY;
-    const int z0 = tz * p.zchunk;         // interior row of the item's first output row
-    const int nrows = min(p.zchunk, nz - z0);
+    const int z0 = tz * g.zchunk;         // interior row of the item's first output row
+    const int nrows = min(g.zchunk, nz - z0);
     const int nsteps = cdiv(nrows, C::ROWS);
     const int nchunks = nsteps + 2 * HCT;
     // array coordinates of input chunk 0
     const int cx = X0 - C::PADL;
     const int cy = Y0 - T_ * C::RY;
     const int cz = hz + z0 - HCT * C::ROWS;
+    double red_acc = 0.0;
 
     // prologue: fill the ring
     const int pre = min(nchunks, C::NSLOT);
     int issued = pre;   // chunks [0, issued) have been issued
     int waited = 0;     // chunks [0, waited) have landed
     for (int k = 0; k < pre; ++k) {
-      const unsigned g = seq + k;
-      const int slot = g % C::NSLOT;
-      Loader<C>::issue(p, ring, ptx::smem_addr(&bars[slot]), slot, cx, cy, cz + k * C::ROWS);
+      const unsigned gq = seq + k;
+      const int slot = gq % C::NSLOT;
+      Loader<C>::issue(g, ring, ptx::smem_addr(&bars[slot]), slot, cx, cy, cz + k * C::ROWS);
     }
 
     for (int i = 0; i < nchunks; ++i) {
       // wait for input chunk i
       {
-        const unsigned g = seq + i;
-        const int slot = g % C::NSLOT;
-        const unsigned parity = (g / C::NSLOT) & 1u;
+        const unsigned gq = seq + i;
+        const int slot = gq % C::NSLOT;
+        const unsigned parity = (gq / C::NSLOT) & 1u;
         if (!ptx::mbar_wait(ptx::smem_addr(&bars[slot]), parity, p.timeout_ns)) {
           abort_flag = 1;
           if (p.err) atomicExch(p.err, CSD_ERR_TIMEOUT);
@@ -330,7 +379,7 @@ __device__ __forceinline__ void stream_engine(const csd_params& p) {
         waited = i;
         if constexpr (C::BC != CSD_BC_NONE) {
           __syncthreads();
-          if (!abort_flag) patch_boundary<C>(p, ring, slot, cx, cy, cz + i * C::ROWS);
+          if (!abort_flag) patch_boundary<C>(g, ring, slot, cx, cy, cz + i * C::ROWS);
         }
       }
       __syncthreads();
@@ -360,6 +409,8 @@ __device__ __forceinline__ void stream_engine(const csd_params& p) {
         }
         src.height = C::H(s - 1);
         src.y_off = C::RY;  // source buffer has RY more rows on each side
+        src.scal = g.scalars;
+        src.dyn = g.dyn;
         const int hs = C::H(s);
         // destination geometry
         const bool last = (s == T_);
@@ -393,12 +444,23 @@ __device__ __forceinline__ void stream_engine(const csd_params& p) {
           const bool yin = gy >= hy && gy < hy + ny;
           if (last) {
             if (!(zin && yin && (zrow0 + r) < z0 + nrows)) continue;
-            const long long rowoff = (long long)gz * p.pitch_z + (long long)gy * p.pitch_y;
+            if constexpr (C::REDUCE) {
+#pragma unroll
+              for (int e = 0; e < C::VEC; ++e) {
+                const int gx = gx0 + e;
+                if (gx >= hx && gx < hx + nx) {
+                  const double v = (double)o.v[0][e];
+                  red_acc = (v != v || v > red_acc) ? v : red_acc;
+                }
+              }
+              continue;
+            }
+            const long long rowoff = (long long)gz * g.pitch_z + (long long)gy * g.pitch_y;
             const bool full = gx0 >= hx && gx0 + C::VEC <= hx + nx;
 #pragma unroll
             for (int f = 0; f < C::NOUT; ++f) {
-              T* out = reinterpret_cast<T*>(p.out[f]) + rowoff;
-              if (full && p.vec_store) {
+              T* out = reinterpret_cast<T*>(g.out[f]) + rowoff;
+              if (full && g.vec_store) {
                 store_vec(out + gx0, o.v[f]);
               } else {
 #pragma unroll
@@ -426,10 +488,10 @@ __device__ __forceinline__ void stream_engine(const csd_params& p) {
         const int dead = i - 2 * C::HC;
         if (dead >= 0 && dead + C::NSLOT < nchunks) {
           const int nk = dead + C::NSLOT;
-          const unsigned g = seq + nk;
-          const int slot = g % C::NSLOT;
+          const unsigned gq = seq + nk;
+          const int slot = gq % C::NSLOT;
           if (C::LOADER == CSD_LOADER_TMA && threadIdx.x == 0) ptx::fence_proxy_async_smem();
-          Loader<C>::issue(p, ring, ptx::smem_addr(&bars[slot]), slot, cx, cy, cz + nk * C::ROWS);
+          Loader<C>::issue(g, ring, ptx::smem_addr(&bars[slot]), slot, cx, cy, cz + nk * C::ROWS);
           issued = nk + 1;
         }
       }
@@ -438,12 +500,27 @@ __device__ __forceinline__ void stream_engine(const csd_params& p) {
       // drain: wait (bounded) for the copies still in flight before leaving
       if (threadIdx.x == 0) {
         for (int k = waited; k < issued; ++k) {
-          const unsigned g = seq + k;
-          ptx::mbar_wait(ptx::smem_addr(&bars[g % C::NSLOT]), (g / C::NSLOT) & 1u, p.timeout_ns);
+          const unsigned gq = seq + k;
+          ptx::mbar_wait(ptx::smem_addr(&bars[gq % C::NSLOT]), (gq / C::NSLOT) & 1u, p.timeout_ns);
         }
       }
       __syncthreads();
       return;
+    }
+    if constexpr (C::REDUCE) {
+      // block max of the item, one atomic per block and item
+      for (int o = 16; o > 0; o >>= 1) {
+        const double w = __shfl_down_sync(0xffffffffu, red_acc, o);
+        red_acc = (w != w || w > red_acc) ? w : red_acc;
+      }
+      if ((threadIdx.x & 31) == 0) red_warp[threadIdx.x >> 5] = red_acc;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double m = red_warp[0];
+        for (int w = 1; w < C::NT / 32; ++w) m = (red_warp[w] != red_warp[w] || red_warp[w] > m) ? red_warp[w] : m;
+        if (g.red) atomic_max_nonneg(g.red, m);
+      }
+      __syncthreads();
     }
     seq += nchunks;
   }

@@ -5,7 +5,8 @@
 #define CSD_PARAMS_H
 
 #define CSD_MAX_FIELDS 8
-#define CSD_DESC_MAGIC 0x43534431u /* "CSD1" */
+#define CSD_MAX_SCALARS 8
+#define CSD_DESC_MAGIC 0x43534432u /* "CSD2" */
 
 #define CSD_LOADER_TMA 0
 #define CSD_LOADER_LDG 1
@@ -27,10 +28,10 @@ typedef struct __attribute__((aligned(64))) csd_tmap {
   unsigned long long opaque[16];
 } csd_tmap;
 
-// Everything a stencil kernel needs at launch.  Arrays are viewed as 3-D
-// (Z, Y, X) with X innermost; a 2-D array (rows, cols) is (rows, 1, cols),
-// a 1-D array (n) is (1, 1, n).  All fields share one shape.
-typedef struct __attribute__((aligned(64))) csd_params {
+// One grid (a set of same-shaped fields) as a kernel sees it.  Arrays are
+// viewed as 3-D (Z, Y, X) with X innermost; a 2-D array (rows, cols) is
+// (rows, 1, cols), a 1-D array (n) is (1, 1, n).
+typedef struct __attribute__((aligned(64))) csd_grid {
   csd_tmap tmap[CSD_MAX_FIELDS];      // TMA descriptors of the inputs
   const void* in[CSD_MAX_FIELDS];     // input base pointers
   void* out[CSD_MAX_FIELDS];          // output base pointers
@@ -44,9 +45,21 @@ typedef struct __attribute__((aligned(64))) csd_params {
   int zchunk;                         // output rows of Z per work item
   int xbase;                          // X origin of tile 0 (halo rounded down to 16 B)
   int vec_store;                      // 1 when 16-byte output stores are aligned
-  int bc_mode;                        // CSD_BC_* applied to the inputs on load
-  int pad0;
-  double bc_value;                    // Dirichlet value for bc_mode
+  int ndim;                           // array dimensionality (1-3)
+  double scalars[CSD_MAX_SCALARS];    // per-grid constants read by the body (s<k>)
+  const double* dyn;                  // per-grid device scalars (d<k>), may be null
+  double* red;                        // per-grid max-reduction slot, may be null
+  double bc_value;                    // Dirichlet value of a fused boundary fill
+  int bc_odd[CSD_MAX_FIELDS];         // bit d: mirrored values of field f flip sign in dim d
+} csd_grid;
+
+// Kernel parameter: one grid inline, or a device array of grids.
+typedef struct __attribute__((aligned(64))) csd_params {
+  csd_grid g;                         // the grid of a single-grid launch
+  const csd_grid* grids;              // batched launch: device array (null otherwise)
+  const int* item_start;              // batched: prefix sums of items, ngrids + 1 entries
+  int ngrids;
+  int total_items;
   int* err;                           // device error word (0 = ok)
   unsigned long long timeout_ns;      // bound on every wait
 } csd_params;
@@ -68,11 +81,14 @@ typedef struct csd_kernel_desc {
   int halo_chunks;
   int pad_left, box_w, box_h;
   int smem_bytes;
-  int zchunk;        // default Z rows per work item
+  int zchunk;        // default Z rows per work item (0 = sized at launch)
   int temporal;      // stencil steps per pass
   int bc_mode;       // CSD_BC_* fused into the staging (0 = none)
   int min_blocks;
   int align;         // elements per 16 bytes
+  int nscalars;      // static per-grid scalars the body reads
+  int ndyn;          // device per-grid scalars the body reads
+  int reduce_max;    // 1: the body also max-reduces a value into grid.red
 } csd_kernel_desc;
 
 #ifdef __cplusplus

@@ -101,6 +101,7 @@ class FuncOp(BuildMixin, Operation):
     boundary = prop()
     constants = prop()
     arg_names = prop()
+    scalar_names = prop()
 
     def __init__(self, func_name, ndim, order, body: Region | Block, input_types=(),
                  output_types=(), dtype=None, boundary=None, constants=None,
@@ -162,19 +163,25 @@ class ComputeOp(BuildMixin, Operation):
 
 
 class YieldOp(BuildMixin, Operation):
-    """Terminator yielding the stencil's point value (dialect.py:345-358)."""
+    """Terminator yielding the stencil's point value(s) (dialect.py:345-358;
+    several values for a tuple-returning body)."""
 
     name = "cutile_stencil.yield"
 
-    def __init__(self, value):
-        super().__init__(operands=[value])
+    def __init__(self, *values):
+        super().__init__(operands=list(values))
 
     @property
     def value(self) -> SSAValue:
         return self.operands[0]
 
+    @property
+    def values(self) -> tuple:
+        return self.operands
+
     def print_custom(self, printer):
-        return f" {printer.print_operand(self.value)} : {self.value.type.print()}"
+        return (" " + ", ".join(printer.print_operand(v) for v in self.operands) + " : "
+                + ", ".join(v.type.print() for v in self.operands))
 
 
 CutileStencilDialect = Dialect("cutile_stencil", [FuncOp, AccessOp, ComputeOp, YieldOp],

@@ -44,6 +44,9 @@ class KernelOp(BuildMixin, Operation):
     layout = prop()
     brick_size = prop()
     boundary_mode = prop()
+    scalar_count = prop()
+    dyn_count = prop()
+    reduce_max = prop()
 
 
 class SliceOp(BuildMixin, Operation):

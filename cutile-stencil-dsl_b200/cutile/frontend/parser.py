@@ -324,6 +324,13 @@ def parse_stencil(fn, ndim: int | None, order: int | None, dtype: str = "float64
         index_vars = params[1:]
     if not index_vars:
         index_vars = [p for p in params if p not in set(array_params)]
+    # Scalar parameters (an extension): parameters that are neither arrays
+    # nor index variables but are read as bare names; their values are given
+    # at launch (per grid) and behave like Python float constants.
+    bare_names = {n.id for root in [return_expr] + [s.value for s in assigns]
+                  for n in ast.walk(root) if isinstance(n, ast.Name)}
+    scalar_params = [p for p in params if p not in set(array_params) and p not in set(index_vars)
+                     and p in bare_names]
 
     # Accesses: the return expression's first, then the assignments'
     # (parser.py:528-535).
@@ -357,6 +364,9 @@ def parse_stencil(fn, ndim: int | None, order: int | None, dtype: str = "float64
     field_args = {}
     for idx, ap in enumerate(array_params):
         field_args[ap] = block.insert_arg(float_type, idx)
+    scalar_args = {}
+    for k, sp in enumerate(scalar_params):
+        scalar_args[sp] = block.insert_arg(f64, len(array_params) + k)
     unique: dict[tuple, SSAValue] = {}
     for name, offsets, node in all_accesses:
         key = (name, tuple(offsets))
@@ -372,12 +382,18 @@ def parse_stencil(fn, ndim: int | None, order: int | None, dtype: str = "float64
 
     builder = _ExprBuilder(block, float_type, unique, all_constants, index_vars,
                            source_file, source_line_offset)
+    builder.locals.update(scalar_args)
     for s in assigns:
         if len(s.targets) != 1 or not isinstance(s.targets[0], ast.Name):
             raise _ParseError("Only simple 'name = expression' assignments are supported")
         builder.locals[s.targets[0].id] = builder.build(s.value)
-    result = builder.build(return_expr)
-    block.add_op(YieldOp(result))
+    if isinstance(return_expr, ast.Tuple):
+        # several outputs from one body (an extension): shared sub-expressions
+        # are evaluated once for all of them
+        results = [builder.build(e) for e in return_expr.elts]
+    else:
+        results = [builder.build(return_expr)]
+    block.add_op(YieldOp(*results))
 
     constants_attr = None
     if all_constants:
@@ -386,6 +402,10 @@ def parse_stencil(fn, ndim: int | None, order: int | None, dtype: str = "float64
     func_op = FuncOp(func_name=func_name, ndim=ndim, order=order, body=Region(block),
                      dtype=dtype, boundary=_boundary_attr(boundary), constants=constants_attr,
                      arg_names=array_params)
+    if scalar_params:
+        from cutile.ir.core import ArrayAttr, StringAttr
+
+        func_op.properties["scalar_names"] = ArrayAttr([StringAttr(n) for n in scalar_params])
     if source_file is not None:
         func_op.location = FileLineColLoc(source_file,
                                           getattr(func_def, "lineno", 0) + source_line_offset,

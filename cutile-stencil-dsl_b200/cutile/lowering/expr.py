@@ -101,14 +101,17 @@ class Program:
         self.expression: str = ""
         self.access_uses: dict[int, int] = {}
         self.extra_returns: list[tuple[str, int]] = []
+        self.n_outputs = 1
 
 
 def build_program(block, access_index: dict, field_dtype: str, spatial_order: bool = False,
-                  access_offsets: dict | None = None) -> Program:
+                  access_offsets: dict | None = None, scalar_args=()) -> Program:
     """Lower the D1 *block* into a :class:`Program`.
 
     ``access_index`` maps each access op result to its index in the kernel's
-    (possibly merged) access list; ``field_dtype`` is ``"f32"`` or ``"f64"``.
+    (possibly merged) access list; ``field_dtype`` is ``"f32"`` or ``"f64"``;
+    ``scalar_args`` are the block arguments of the stencil's scalar
+    parameters (operands ``s<k>``: Python floats given at launch).
     """
     prog = Program()
     const: dict = {}     # value -> python float (folded constants)
@@ -116,6 +119,10 @@ def build_program(block, access_index: dict, field_dtype: str, spatial_order: bo
     name: dict = {}      # value -> SSA operand name
     infix: dict = {}     # value -> readable expression
     counter = [0]
+    for k, arg in enumerate(scalar_args):
+        name[arg] = f"s{k}"
+        vtype[arg] = "w"
+        infix[arg] = f"s{k}"
 
     def new(line_rhs: str, t: str) -> str:
         n = f"v{counter[0]}"
@@ -235,11 +242,21 @@ def build_program(block, access_index: dict, field_dtype: str, spatial_order: bo
             infix[op.result] = f"where({text(c)}, {text(a)}, {text(b)})"
         elif isinstance(op, YieldOp):
             result_value = op.value
+            yields = list(op.values)
         else:
             raise ValueError(f"unsupported op in stencil body: {op.name}")
 
     if result_value is None:
         raise ValueError("stencil body has no yield")
+    if len(yields) > 1:
+        # tuple-returning body: one output per element, in order
+        for i, v in enumerate(yields):
+            prog.extra_returns.append((operand(v), i))
+        prog.result = prog.extra_returns[0][0]
+        prog.result_type = vtype[yields[0]]
+        prog.expression = "(" + ", ".join(text(v) for v in yields) + ")"
+        prog.n_outputs = len(yields)
+        return prog
     if spatial_order and access_offsets:
         # Opt-in re-association of a top-level sum in spatial access order
         # (the reference's default above 64 loads, stencil_to_target.py:443-448).

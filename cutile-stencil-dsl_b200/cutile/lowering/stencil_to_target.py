@@ -80,10 +80,20 @@ class _StencilMeta:
         self.stencil_inputs: list[list[str]] = []
         self.programs: list[Program] = []
         self.kahan = False
+        self.scalar_names: list[str] = []
+        self.rk_stage = None
+        self.dyn_count = 0
+        self.reduce_max = False
 
     @property
     def num_outputs(self) -> int:
-        return max(1, len(self.expressions)) * (2 if self.kahan else 1)
+        if self.programs and len(self.programs) == 1 and self.programs[0].n_outputs > 1:
+            n = self.programs[0].n_outputs
+        else:
+            n = max(1, len(self.expressions))
+        if self.rk_stage is not None:
+            return n * (2 if self.rk_stage.get("w") is not None else 1)
+        return n * (2 if self.kahan else 1)
 
     def output_views(self) -> list[str]:
         if self.num_outputs == 1:
@@ -91,6 +101,8 @@ class _StencilMeta:
         return [f"out_{k}" for k in range(self.num_outputs)]
 
     def output_params(self) -> list[str]:
+        if self.rk_stage is not None or (self.programs and self.programs[0].n_outputs > 1):
+            return [f"out{k}" for k in range(self.num_outputs)]
         if self.output_names:
             outs = [f"{n}_out" for n in self.output_names]
             return outs + [f"{n}_c_out" for n in self.output_names] if self.kahan else outs
@@ -186,7 +198,9 @@ def _extract_meta(func_op: FuncOp, block: Block, spatial_term_order: bool | None
         meta.dtype = func_op.dtype.data
     if dtype is not None:
         meta.dtype = dtype
-    meta.num_inputs = len(block.args)
+    n_scalars = len(func_op.scalar_names.data) if func_op.scalar_names is not None else 0
+    meta.scalar_names = [a.data for a in func_op.scalar_names.data] if n_scalars else []
+    meta.num_inputs = len(block.args) - n_scalars
     if input_names is not None:
         if len(input_names) != meta.num_inputs:
             raise ValueError(f"{meta.name}: {len(input_names)} input names for "
@@ -225,7 +239,8 @@ def _extract_meta(func_op: FuncOp, block: Block, spatial_term_order: bool | None
     if spatial_term_order is None:
         spatial_term_order = False
     prog = build_program(block, access_index, _field_dtype(meta.dtype),
-                         spatial_order=bool(spatial_term_order), access_offsets=access_offsets)
+                         spatial_order=bool(spatial_term_order), access_offsets=access_offsets,
+                         scalar_args=block.args[meta.num_inputs:])
     meta.programs = [prog]
     meta.expression = prog.expression
     meta.expressions = [meta.expression]
@@ -313,6 +328,100 @@ def apply_kahan(meta: _StencilMeta, comp_names: Sequence[str] | None = None) -> 
     return meta
 
 
+def apply_rk_stage(meta: _StencilMeta, a: float, b: float, c: float, w: float | None = None,
+                   same_base: bool = False) -> _StencilMeta:
+    """Turn the operator ``L`` (one derivative per state field, the first
+    ``M`` array parameters) into one fused Runge-Kutta stage:
+
+        next_m = a * base_m + b * stage_m + (c * dt) * L_m(stage)
+        acc_m  = acc_m + (w * dt) * L_m(stage)            (only when w is given)
+
+    evaluated in FP64 with round-to-nearest operations in that order and
+    rounded once to the field dtype; ``dt`` is the per-grid device scalar
+    ``d0``; terms with a zero coefficient are not emitted.  Inputs become the
+    operator's inputs (the stage state), then ``base_m`` (if ``a`` and the
+    base is not the stage state itself, ``same_base``), then ``acc_m`` (if
+    ``w``); outputs ``next_m`` then ``acc_m``.
+    """
+    if len(meta.programs) != 1:
+        raise ValueError("Runge-Kutta stages take a single operator stencil")
+    prog = meta.programs[0]
+    m_count = prog.n_outputs
+    if m_count > meta.num_inputs:
+        raise ValueError("the operator returns more derivatives than it has fields")
+    rets = prog.extra_returns or [(prog.result, 0)]
+    zeros = (0,) * meta.ndim
+    center = {a_.array_index: j for j, a_ in enumerate(meta.accesses) if not any(a_.offsets)}
+    st = _field_dtype(meta.dtype)
+    lines = list(prog.lines)
+    counter = [0]
+
+    def new(rhs, t="f64"):
+        n = f"r{counter[0]}"
+        counter[0] += 1
+        lines.append(f"{n} = {rhs} : {t}")
+        return n
+
+    def add_input(prefix, m):
+        meta.input_names.append(f"{prefix}_{meta.input_names[m]}")
+        j = len(meta.accesses)
+        meta.accesses.append(_AccessInfo(len(meta.input_names) - 1, zeros,
+                                         f"{meta.input_names[-1]}_0_0"))
+        return f"a{j}"
+
+    def center_of(m):
+        if m not in center:
+            j = len(meta.accesses)
+            meta.accesses.append(_AccessInfo(m, zeros, f"{meta.input_names[m]}_0_0"))
+            center[m] = j
+        return f"a{center[m]}"
+
+    stage_c = {m: center_of(m) for m in range(m_count)} if (b != 0.0 or same_base) else {}
+    n_ops = meta.num_inputs
+    if a != 0.0:
+        base_a = ({m: stage_c[m] for m in range(m_count)} if same_base else
+                  {m: add_input("base", m) for m in range(m_count)})
+    else:
+        base_a = {}
+    acc_a = {m: add_input("acc", m) for m in range(m_count)} if w is not None else {}
+    del n_ops
+    new_rets = []
+    kc = new(f"const {float(c)!r}", "w")
+    cdt = new(f"mulf {kc}, d0", "w")
+    kw = None
+    if w is not None:
+        kw = new(f"mulf {new(f'const {float(w)!r}', 'w')}, d0", "w")
+    for m, (lv, _) in enumerate(rets):
+        L = new(f"cast {lv}")
+        term = new(f"mulf {cdt}, {L}")
+        x = None
+        if a != 0.0:
+            base = new(f"cast {base_a[m]}")
+            x = base if a == 1.0 else new(f"mulf {new(f'const {float(a)!r}', 'w')}, {base}")
+        if b != 0.0:
+            sv = new(f"cast {stage_c[m]}")
+            y = sv if b == 1.0 else new(f"mulf {new(f'const {float(b)!r}', 'w')}, {sv}")
+            x = y if x is None else new(f"addf {x}, {y}")
+        x = term if x is None else new(f"addf {x}, {term}")
+        nxt = new(f"cast {x}", st)
+        new_rets.append((nxt, m))
+        if w is not None:
+            accv = new(f"cast {acc_a[m]}")
+            upd = new(f"addf {accv}, {new(f'mulf {kw}, {L}')}")
+            new_rets.append((new(f"cast {upd}", st), m_count + m))
+    prog.lines = lines
+    prog.extra_returns = new_rets
+    prog.result = new_rets[0][0]
+    prog.n_outputs = m_count
+    meta.num_inputs = len(meta.input_names)
+    meta.rk_stage = {"a": a, "b": b, "c": c, "w": w}
+    meta.dyn_count = 1
+    prog.expression = f"rk_stage(a={a}, b={b}, c={c}, w={w}; {prog.expression})"
+    meta.expressions = [prog.expression]
+    meta.expression = prog.expression
+    return meta
+
+
 def _owners(shared, metas):
     done = set()
     for m in metas:
@@ -389,6 +498,9 @@ def _build_kernel_op(meta: _StencilMeta, tile_sizes: tuple[int, ...], halo_width
         "layout": StringAttr(layout),
         "brick_size": IntAttr(brick_size),
         "boundary_mode": StringAttr(boundary_mode),
+        "scalar_count": IntAttr(len(meta.scalar_names)),
+        "dyn_count": IntAttr(meta.dyn_count),
+        "reduce_max": IntAttr(1 if meta.reduce_max else 0),
     }
     if meta.num_outputs > 1:
         props["expressions"] = ArrayAttr([StringAttr(x) for x in meta.expressions])
@@ -444,12 +556,25 @@ def lower_to_target_ir(module: ModuleOp, tile_sizes: tuple[int, ...], halo_width
                        temporal_steps: int = 1, boundary_spec: dict | None = None,
                        kernel_hints: dict | None = None, spatial_term_order: bool | None = None,
                        *, dtype: str | None = None, layout: str = "flat", brick_size: int = 0,
-                       boundary_mode: str = "none", kahan: bool = False) -> ModuleOp:
-    """Dialect 1 module -> Dialect 3 module (``cutile.kernel`` + host program)."""
+                       boundary_mode: str = "none", kahan: bool = False, rk: dict | None = None,
+                       reduce_max: bool = False, name: str | None = None) -> ModuleOp:
+    """Dialect 1 module -> Dialect 3 module (``cutile.kernel`` + host program).
+
+    Variants: ``kahan`` (compensated FP32 update), ``rk`` (a Runge-Kutta stage
+    with coefficients ``a, b, c[, w]``, see ``apply_rk_stage``), ``reduce_max``
+    (the body's value is max-reduced per grid instead of stored)."""
     func_op, block = _func_and_block(module)
     meta = _extract_meta(func_op, block, spatial_term_order, dtype=dtype)
     if kahan:
         apply_kahan(meta)
+    if rk is not None:
+        apply_rk_stage(meta, rk["a"], rk["b"], rk["c"], rk.get("w"), rk.get("same_base", False))
+    if reduce_max:
+        if meta.num_outputs != 1:
+            raise ValueError("a max-reduction takes a single-valued body")
+        meta.reduce_max = True
+    if name is not None:
+        meta.name = name
     if boundary_spec is None and meta.boundary is not None:
         boundary_spec = meta.boundary
     kernel = _build_kernel_op(meta, tile_sizes, halo_widths, kernel_hints,

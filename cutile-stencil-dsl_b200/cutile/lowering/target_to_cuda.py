@@ -84,7 +84,8 @@ class _BodyEmitter:
         self.lines: list[str] = []
 
     def name(self, v: str) -> str:
-        return v if v.startswith("a") else f"{self.prefix}{v}"
+        # accesses a<j>, scalars s<k> and device scalars d<k> are shared names
+        return v if v[0] in "asd" else f"{self.prefix}{v}"
 
     def conv(self, v: str, to: str) -> str:
         """Operand *v* as C type of numpy kind *to* (f32/f64)."""
@@ -179,14 +180,22 @@ def emit_body(kernel: KernelOp) -> str:
     for gi, key in enumerate(gkeys):
         f, dz, dy = key
         lo, hi = min(groups[key]), max(groups[key])
-        out.append(f"    const auto s{gi} = t.template strip<{f}, {dz}, {dy}, {lo}, {hi}>(r, y, x);")
+        out.append(f"    const auto st{gi} = t.template strip<{f}, {dz}, {dy}, {lo}, {hi}>(r, y, x);")
+    access_types = {}
+    n_scal = kernel.scalar_count.data if kernel.scalar_count is not None else 0
+    n_dyn = kernel.dyn_count.data if kernel.dyn_count is not None else 0
+    for k in range(n_scal):
+        out.append(f"    const double s{k} = t.scalar({k});")
+        access_types[f"s{k}"] = "w"
+    for k in range(n_dyn):
+        out.append(f"    const double d{k} = t.dynamic({k});")
+        access_types[f"d{k}"] = "w"
     out.append("#pragma unroll")
     out.append("    for (int k = 0; k < C::VEC; ++k) {")
-    access_types = {}
     for j, (key, dx) in enumerate(acc_info):
         gi = gkeys.index(key)
         lo = min(groups[key])
-        out.append(f"      const {store_t} a{j} = s{gi}.v[k + {dx - lo}];")
+        out.append(f"      const {store_t} a{j} = st{gi}.v[k + {dx - lo}];")
         access_types[f"a{j}"] = field_t
     for m, prog in enumerate(kernel.ssa_body.data):
         em = _BodyEmitter(f"p{m}_")
@@ -238,8 +247,11 @@ def engine_params(kernel: KernelOp) -> dict:
         "NT": int(hints.get("threads", 256)), "STAGES": int(hints.get("stages", 1)),
         "TEMPORAL": kernel.temporal_steps.data if kernel.temporal_steps is not None else 1,
         "BC": BC_CODES[kernel.boundary_mode.data if kernel.boundary_mode is not None else "none"],
-        "MINB": int(hints.get("min_blocks", 1)), "ZCHUNK": int(hints.get("zchunk", 64)),
+        "MINB": int(hints.get("min_blocks", 1)), "ZCHUNK": int(hints.get("zchunk", 0)),
         "ndim": ndim,
+        "NSCAL": kernel.scalar_count.data if kernel.scalar_count is not None else 0,
+        "NDYN": kernel.dyn_count.data if kernel.dyn_count is not None else 0,
+        "REDUCE": kernel.reduce_max.data if kernel.reduce_max is not None else 0,
     }
 
 
@@ -270,7 +282,7 @@ def emit_cuda(module: ModuleOp, preamble: bool = True) -> str:
         for suffix, loader in (("tma", "CSD_LOADER_TMA"), ("ldg", "CSD_LOADER_LDG")):
             cfg = (f"csd::Cfg<{p['T']}, {p['NIN']}, {p['NOUT']}, {p['RZ']}, {p['RY']}, {p['RX']}, "
                    f"{p['ROWS']}, {p['TY']}, {p['TX']}, {p['NT']}, {p['STAGES']}, {p['TEMPORAL']}, "
-                   f"{loader}, {p['BC']}>")
+                   f"{loader}, {p['BC']}, {p['REDUCE']}>")
             parts.append(f"typedef {cfg} Cfg_{name}_{suffix};")
             parts.append(f'extern "C" __global__ void __launch_bounds__({p["NT"]}, {p["MINB"]})')
             parts.append(f"{name}_{suffix}(const __grid_constant__ csd_params p) {{")
@@ -278,11 +290,13 @@ def emit_cuda(module: ModuleOp, preamble: bool = True) -> str:
             parts.append("}")
         c = f"Cfg_{name}_tma"
         parts.append(f'extern "C" __device__ const csd_kernel_desc {name}_desc = {{')
-        parts.append(f"  CSD_DESC_MAGIC, {p['ndim']}, {c}::NIN, {c}::NOUT, (int)sizeof({c}::T),")
+        nout_desc = "0" if p["REDUCE"] else f"{c}::NOUT"
+        parts.append(f"  CSD_DESC_MAGIC, {p['ndim']}, {c}::NIN, {nout_desc}, (int)sizeof({c}::T),")
         parts.append(f"  {c}::RZ * {c}::TEMPORAL, {c}::RY * {c}::TEMPORAL, {c}::RX * {c}::TEMPORAL,")
         parts.append(f"  {c}::ROWS, {c}::TY, {c}::TX, {c}::VEC, {c}::NT, {c}::STAGES, {c}::NSLOT,")
         parts.append(f"  {c}::HC * {c}::TEMPORAL, {c}::PADL, {c}::BOXW, {c}::BOXH, {c}::SMEM_BYTES,")
-        parts.append(f"  {p['ZCHUNK']}, {c}::TEMPORAL, {c}::BC, {p['MINB']}, {c}::ALIGN}};")
+        parts.append(f"  {p['ZCHUNK']}, {c}::TEMPORAL, {c}::BC, {p['MINB']}, {c}::ALIGN,")
+        parts.append(f"  {p['NSCAL']}, {p['NDYN']}, {p['REDUCE']}}};")
         parts.append("")
     return "\n".join(parts) + "\n"
 

@@ -48,20 +48,23 @@ class NormalizePass(ModulePass):
         dtype_str = d1.dtype.data if d1.dtype is not None else "float64"
         float_type = f32 if dtype_str == "float32" else f64
         d1_body = d1.body.blocks[0]
-        num_arrays = len(d1_body.args)
+        n_scalars = len(d1.scalar_names.data) if d1.scalar_names is not None else 0
+        num_arrays = len(d1_body.args) - n_scalars
         temp_type = TempType(ndim, float_type)
 
         block = Block()
         vmap = {}
         for idx in range(num_arrays):
             vmap[d1_body.args[idx]] = block.insert_arg(temp_type, idx)
+        for k in range(n_scalars):
+            vmap[d1_body.args[num_arrays + k]] = block.insert_arg(f64, num_arrays + k)
         for op in d1_body.ops:
             if isinstance(op, D1AccessOp):
                 new = StdAccessOp(vmap[op.field], list(op.offset.offsets))
                 block.add_op(new)
                 vmap[op.res] = new.res
             elif isinstance(op, D1YieldOp):
-                block.add_op(ReturnOp([vmap[op.value]]))
+                block.add_op(ReturnOp([vmap[v] for v in op.values]))
             else:
                 new = op.clone(vmap)
                 block.add_op(new)

@@ -246,7 +246,7 @@ def radius3(ndim: int, radius: tuple[int, ...]) -> tuple[int, int, int]:
 
 
 def fit_plan(plan: EnginePlan, radius: tuple[int, ...], dtype_bytes: int,
-             num_inputs: int) -> EnginePlan:
+             num_inputs: int, body_ops: int = 0) -> EnginePlan:
     """Shrink a plan until its TMA box and shared memory fit the B200 limits."""
     r3 = radius3(plan.ndim, radius)
     for _ in range(64):
@@ -272,9 +272,11 @@ def fit_plan(plan: EnginePlan, radius: tuple[int, ...], dtype_bytes: int,
     zchunk = 0 if plan.zchunk <= 0 else max(plan.rows, (plan.zchunk // plan.rows) * plan.rows)
     g = engine_geometry(plan, r3, dtype_bytes, num_inputs)
     # resident blocks the shared memory allows, capped so the register budget
-    # stays >= 64 per thread (the launch bound is a hint to ptxas, not a floor)
+    # stays >= 64 per thread (128 for long bodies such as flux stencils, which
+    # otherwise spill); the launch bound is a hint to ptxas, not a floor
+    regs = 128 if body_ops > 120 else 64
     min_blocks = max(1, min(B200_SMEM_PER_SM // max(1, g["smem_bytes"] + 1024),
-                            B200_MAX_THREADS_PER_SM // threads, 65536 // (threads * 64)))
+                            B200_MAX_THREADS_PER_SM // threads, 65536 // (threads * regs)))
     return replace(plan, threads=threads, zchunk=zchunk, min_blocks=min_blocks)
 
 

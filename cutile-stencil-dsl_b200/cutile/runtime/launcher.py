@@ -232,7 +232,8 @@ def _num_inputs(ir) -> int:
 
     for op in ir.body.block.ops:
         if isinstance(op, FuncOp):
-            return len(op.body.blocks[0].args)
+            n_scalars = len(op.scalar_names.data) if op.scalar_names is not None else 0
+            return len(op.body.blocks[0].args) - n_scalars
     return 1
 
 
@@ -294,13 +295,16 @@ def generate_module_code(name: str, cuda_source: str, spec: dict, *, fused_outpu
     e.line("_PROGRAM = StencilProgram(CUDA_SOURCE, SPEC)")
     inputs = spec["input_names"]
     outs = spec["output_params"]
+    scal = spec.get("scalars", [])
+    kw = (", *, " + ", ".join(scal)) if scal else ""
+    sc = ("{" + ", ".join(f"{n!r}: {n}" for n in scal) + "}") if scal else "None"
     e.blank()
     e.blank()
     args = ", ".join(inputs + outs)
-    e.line(f"def launch_{name}({args}, stream=None):")
+    e.line(f"def launch_{name}({args}, stream=None{kw}):")
     with e.indent():
         e.line(f'"""{spec["temporal_steps"]} step(s) of {name}; writes the interior of the output(s)."""')
-        e.line(f"_PROGRAM.launch(({', '.join(inputs)},), ({', '.join(outs)},), stream)")
+        e.line(f"_PROGRAM.launch(({', '.join(inputs)},), ({', '.join(outs)},), stream, scalars={sc})")
     if spec.get("boundary") is not None:
         e.blank()
         e.blank()
@@ -310,10 +314,10 @@ def generate_module_code(name: str, cuda_source: str, spec: dict, *, fused_outpu
             e.line("_PROGRAM.apply_boundary(u, stream)")
         e.blank()
         e.blank()
-        e.line(f"def step_{name}({args}, stream=None):")
+        e.line(f"def step_{name}({args}, stream=None{kw}):")
         with e.indent():
             e.line('"""One step with the boundary condition fused into the staging."""')
-            e.line(f"_PROGRAM.step(({', '.join(inputs)},), ({', '.join(outs)},), stream)")
+            e.line(f"_PROGRAM.step(({', '.join(inputs)},), ({', '.join(outs)},), stream, scalars={sc})")
     e.blank()
     e.blank()
     e.line("def program():")
@@ -326,6 +330,7 @@ def generate_module_code(name: str, cuda_source: str, spec: dict, *, fused_outpu
 def _analysis_of(clone) -> tuple:
     halo_widths, tile_sizes, temporal_steps = (1,), (256,), 1
     analysis, occupancy, num_loads = {}, None, 0
+    body_ops = 0
     from cutile.passes.tiling import unique_access_count
 
     for op in clone.walk():
@@ -340,10 +345,12 @@ def _analysis_of(clone) -> tuple:
             if "occupancy" in a:
                 occupancy = a["occupancy"].data
             num_loads = unique_access_count(op)
+            body_ops = sum(1 for _ in op.region.walk())
             for key in ("flops", "unique_loads", "arithmetic_intensity", "bound"):
                 if key in a:
                     analysis[key] = a[key].data
             break
+    analysis["body_ops"] = body_ops
     return halo_widths, tile_sizes, temporal_steps, analysis, occupancy, num_loads
 
 
@@ -354,13 +361,18 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
             occupancy: int | None = None, select: str | None = None, *,
             temporal_steps: int | None = None, tile_sizes: tuple[int, ...] | None = None,
             kernel_hints: dict | None = None, dtype: str | None = None,
-            precision: str | None = None) -> CompileResult:
+            precision: str | None = None, reduce: str | None = None) -> CompileResult:
     """Compile a ``@stencil`` function for the B200 engine (launcher.py:342-602).
 
     ``precision`` (extension): ``"fp64"``, ``"fp32"`` or ``"fp32_kahan"`` --
     the last stores fields in FP32 and applies the body, which must read
     ``u + increment``, as a Kahan-compensated update with a compensation field
-    (``launch_<name>(u_in, c_in, u_out, c_out)``)."""
+    (``launch_<name>(u_in, c_in, u_out, c_out)``).  ``reduce="max"``
+    (extension) compiles a pointwise body whose values are max-reduced per
+    grid into a device scalar (``reduce_<name>(inputs..., out=None)``)."""
+    if reduce is not None:
+        return _compile_reduction(stencil_fn, reduce, dtype=dtype, precision=precision,
+                                  align_halo=align_halo)
     from cutile.lowering.stencil_to_target import lower_to_target_ir
     from cutile.lowering.target_to_cuda import emit_cuda
     from cutile.passes.tiling import default_engine_plan, fit_plan
@@ -402,13 +414,13 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
         T = int(temporal_steps)
         if T > 1 and num_inputs != 1:
             raise NotImplementedError("temporal blocking needs a single-field stencil")
-    elif num_inputs != 1:
+    elif num_inputs != 1 or _yields(ir) > 1:
         # The reference's T-launch loop chains one field only
         # (stencil_to_target.py:796-800), so a multi-field stencil cannot run
         # blocked there either; it advances one step per launch.
         T = 1
     plan = _plan_from(tile_sizes, kernel_hints, len(stencil_halo), replace(plan, temporal=T))
-    plan = fit_plan(plan, stencil_halo, dtype_bytes, num_inputs)
+    plan = fit_plan(plan, stencil_halo, dtype_bytes, num_inputs, analysis.get("body_ops", 0))
     hints = plan.hints()
     if occupancy is not None:
         hints["occupancy"] = occupancy
@@ -440,7 +452,8 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
     multi = n_fields > 1
     names = ([n for n in "uvwxyz"][:n_fields] if n_fields <= 6 else
              [f"arr{i}" for i in range(n_fields)]) if multi else ["u_in"]
-    outs = ["u_out"]
+    n_out = _kernel_outputs(target)
+    outs = ["u_out"] if n_out == 1 else [f"out{k}" for k in range(n_out)]
     if kahan:
         names = names + ["c_in"]
         outs = ["u_out", "c_out"]
@@ -450,6 +463,7 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
         "temporal_steps": T, "boundary": boundary_spec, "kernels": kernels,
         "input_names": names, "output_params": outs, "zchunk": plan.zchunk,
         "precision": precision or ("fp32" if dtype == "float32" else "fp64"),
+        "scalars": _scalar_names(ir),
     }
     code = generate_module_code(name, cuda, spec)
     return CompileResult(
@@ -460,6 +474,34 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
         dtype=dtype,
         boundary=boundary_spec, layout=layout or "flat", brick_size=brick_size if layout == "bricked" else 0,
         _ref_fn=stencil_fn._fn, _ref_fns=[stencil_fn._fn])
+
+
+def _yields(ir) -> int:
+    from cutile.dialects.cutile_stencil.dialect import YieldOp
+    from cutile.lowering.stencil_to_target import _func_and_block
+
+    _, b = _func_and_block(ir)
+    for op in b.ops:
+        if isinstance(op, YieldOp):
+            return len(op.operands)
+    return 1
+
+
+def _kernel_outputs(target) -> int:
+    from cutile.dialects.cutile_target import KernelOp
+
+    for op in target.body.block.ops:
+        if isinstance(op, KernelOp):
+            return sum(max(1, sum(1 for x in prog if x.data.startswith("return")))
+                       for prog in op.ssa_body.data)
+    return 1
+
+
+def _scalar_names(ir) -> list:
+    from cutile.lowering.stencil_to_target import _func_and_block
+
+    f, _ = _func_and_block(ir)
+    return [a.data for a in f.scalar_names.data] if f.scalar_names is not None else []
 
 
 def _rename_kernel(target, new_name: str) -> None:
@@ -560,3 +602,109 @@ def compile_fused(stencil_fns: list, domain: tuple[int, ...] | None = None, hw=N
 
 __all__ = ["compile", "compile_fused", "CompileResult", "pad_inner_halo",
            "generate_module_code"]
+
+
+# --------------------------------------------------------------------------- #
+# Kernel variants (Runge-Kutta stages, reductions) of one stencil
+# --------------------------------------------------------------------------- #
+
+
+def build_variants(stencil_fn, variants: dict, *, dtype: str | None = None,
+                   precision: str | None = None, align_halo: bool = True,
+                   tile_sizes=None, kernel_hints=None, boundary=None):
+    """Lower several kernel variants of one stencil into one CUDA unit.
+
+    ``variants`` maps a kernel name to options for ``lower_to_target_ir``
+    (``rk=``, ``reduce_max=``, ``boundary_mode=``).  Returns
+    ``(cuda_source, info)`` with the halo (padded and stencil), the engine plan
+    and, per kernel, its input and output counts.
+    """
+    from cutile.lowering.stencil_to_target import lower_to_target_ir
+    from cutile.lowering.target_to_cuda import emit_cuda, engine_params
+    from cutile.passes.tiling import default_engine_plan, fit_plan
+
+    ir = stencil_fn._ir
+    dtype, _ = _precision(precision, dtype or getattr(stencil_fn, "_dtype", "float64"))
+    dtype_bytes = 4 if dtype == "float32" else 8
+    clone = ir.clone()
+    Pipeline.single_gpu(dtype_bytes=dtype_bytes, max_temporal_steps=1).run(clone)
+    stencil_halo, _t, _T, analysis, _o, num_loads = _analysis_of(clone)
+    halo_widths = pad_inner_halo(stencil_halo, dtype_bytes) if align_halo else stencil_halo
+    n_fields = _num_inputs(ir)
+    parts = []
+    info = {"halo": tuple(halo_widths), "stencil_halo": tuple(stencil_halo), "dtype": dtype,
+            "kernels": {}, "scalars": _scalar_names(ir), "analysis": analysis}
+    bspec = None
+    if boundary is not None:
+        bspec = {"type": boundary} if isinstance(boundary, str) else dict(boundary)
+    first = True
+    for kname, opts in variants.items():
+        opts = dict(opts)
+        extra_in = 0
+        if opts.get("rk") is not None:
+            rk = opts["rk"]
+            m = _yields(ir)
+            extra_in = ((m if rk["a"] != 0.0 and not rk.get("same_base") else 0)
+                        + (m if rk.get("w") is not None else 0))
+        plan = default_engine_plan(len(stencil_halo), num_loads, dtype_bytes, stencil_halo,
+                                   n_fields + extra_in)
+        plan = fit_plan(_plan_from(tile_sizes, kernel_hints, len(stencil_halo), plan),
+                        stencil_halo, dtype_bytes, n_fields + extra_in,
+                        analysis.get("body_ops", 0))
+        bmode = opts.pop("boundary_mode", "none")
+        target = lower_to_target_ir(ir.clone(), plan.tile_sizes(), tuple(halo_widths),
+                                    kernel_hints=plan.hints(), dtype=dtype, name=kname,
+                                    boundary_spec=bspec, boundary_mode=bmode, **opts)
+        parts.append(emit_cuda(target, preamble=first))
+        first = False
+        from cutile.dialects.cutile_target import KernelOp
+
+        kop = next(op for op in target.body.block.ops if isinstance(op, KernelOp))
+        ep = engine_params(kop)
+        info["kernels"][kname] = {"inputs": ep["NIN"], "outputs": 0 if ep["REDUCE"] else ep["NOUT"],
+                                  "plan": plan}
+    return "\n".join(parts), info
+
+
+def _compile_reduction(stencil_fn, reduce: str, *, dtype=None, precision=None,
+                       align_halo=True) -> CompileResult:
+    from cutile.lowering.emitter import CodeEmitter
+
+    if reduce != "max":
+        raise ValueError("only reduce='max' is supported (non-negative values, NaN propagates)")
+    name = stencil_fn._fn.__name__
+    cuda, info = build_variants(stencil_fn, {name: {"reduce_max": True}}, dtype=dtype,
+                                precision=precision, align_halo=align_halo)
+    n_in = info["kernels"][name]["inputs"]
+    names = [f"u{k}" for k in range(n_in)] if n_in > 1 else ["u_in"]
+    spec = {"name": name, "ndim": len(info["halo"]), "dtype": info["dtype"],
+            "halo": list(info["halo"]), "stencil_halo": list(info["stencil_halo"]),
+            "inputs": n_in, "outputs": 0, "temporal_steps": 1, "boundary": None,
+            "kernels": {"main": name}, "input_names": names, "output_params": [],
+            "zchunk": 0, "scalars": info["scalars"], "reduce": "max"}
+    e = CodeEmitter()
+    e.line(f'"""Per-grid max of {name} over the interior (generated)."""')
+    e.blank()
+    e.line("from cutile.runtime.module import StencilProgram")
+    e.blank()
+    e.line("CUDA_SOURCE = r\'\'\'" + cuda + "\'\'\'")
+    e.line(f"SPEC = {spec!r}")
+    e.line("SPEC['halo'] = tuple(SPEC['halo'])")
+    e.line("_PROGRAM = StencilProgram(CUDA_SOURCE, SPEC)")
+    e.blank()
+    e.blank()
+    e.line(f"def reduce_{name}({', '.join(names)}, out=None, stream=None, **scalars):")
+    with e.indent():
+        e.line('"""Max over the interior into the device float64 ``out`` (returned);'
+               ' the value is max(out, ...) when ``out`` is given."""')
+        e.line(f"return _PROGRAM.reduce(({', '.join(names)},), out, stream, scalars)")
+    e.blank()
+    e.blank()
+    e.line("def program():")
+    with e.indent():
+        e.line("return _PROGRAM")
+    return CompileResult(name=name, code=e.render(), ndim=len(info["halo"]),
+                         halo_widths=tuple(info["halo"]), tile_sizes=(), temporal_steps=1,
+                         analysis=info["analysis"], stencil_halo=tuple(info["stencil_halo"]),
+                         inputs=_input_names(stencil_fn._ir), cuda_source=cuda,
+                         dtype=info["dtype"], _ref_fn=stencil_fn._fn, _ref_fns=[stencil_fn._fn])

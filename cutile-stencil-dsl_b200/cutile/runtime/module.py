@@ -75,8 +75,20 @@ class StencilProgram:
                 raise ValueError(f"{self.spec['name']}: extent {n} leaves no interior with halo {h}")
 
     # -- entry points --------------------------------------------------------
+    def scalar_values(self, scalars: dict | None) -> list:
+        names = self.spec.get("scalars", [])
+        scalars = scalars or {}
+        missing = [n for n in names if n not in scalars]
+        if missing:
+            raise TypeError(f"{self.spec['name']}: missing scalar parameter(s) {missing}")
+        extra = set(scalars) - set(names)
+        if extra:
+            raise TypeError(f"{self.spec['name']}: unknown scalar parameter(s) {sorted(extra)}")
+        return [float(scalars[n]) for n in names]
+
     def launch(self, inputs, outputs, stream=None, *, zchunk: int = 0, grid: int = 0,
-               loader: int = -1) -> None:
+               loader: int = -1, scalars: dict | None = None, which: str = "main",
+               dyn=None, red=None, bc_odd=()) -> None:
         """``launch_<name>``: ``temporal_steps`` steps from ``inputs`` into the
         interiors of ``outputs`` (halos untouched)."""
         self._check(list(inputs) + list(outputs), "stencil")
@@ -87,10 +99,11 @@ class StencilProgram:
             for i in inputs:
                 if o.data_ptr() == i.data_ptr():
                     raise ValueError("outputs must not alias inputs (the kernel reads neighbours)")
-        native.launch(self.kernel("main"), inputs, outputs, self.spec["halo"], stream,
-                      zchunk=zchunk, grid=grid, loader=loader)
+        native.launch(self.kernel(which), inputs, outputs, self.spec["halo"], stream,
+                      zchunk=zchunk, grid=grid, loader=loader,
+                      scalars=self.scalar_values(scalars), dyn=dyn, red=red, bc_odd=bc_odd)
 
-    def step(self, inputs, outputs, stream=None, **kw) -> None:
+    def step(self, inputs, outputs, stream=None, *, scalars: dict | None = None, **kw) -> None:
         """One step with the declared boundary condition fused into staging:
         ``out = stencil(apply_boundary(in))`` without writing the inputs' halos."""
         if "fused_bc" not in self.spec["kernels"]:
@@ -98,7 +111,19 @@ class StencilProgram:
         self._check(list(inputs) + list(outputs), "stencil")
         bc = self.spec["boundary"] or {}
         native.launch(self.kernel("fused_bc"), inputs, outputs, self.spec["halo"], stream,
-                      bc_value=float(bc.get("value", 0.0)), **kw)
+                      bc_value=float(bc.get("value", 0.0)),
+                      scalars=self.scalar_values(scalars), **kw)
+
+    def reduce(self, inputs, out=None, stream=None, scalars: dict | None = None):
+        """Max-reduce the body over the interior into the device scalar ``out``."""
+        import torch
+
+        self._check(list(inputs), "reduction")
+        if out is None:
+            out = torch.zeros((), dtype=torch.float64, device=inputs[0].device)
+        native.launch(self.kernel("main"), inputs, [], self.spec["halo"], stream,
+                      scalars=self.scalar_values(scalars), red=out)
+        return out
 
     def apply_boundary(self, u, stream=None) -> None:
         """``apply_boundary_<name>(u)``: fill the halo of ``u`` in place."""

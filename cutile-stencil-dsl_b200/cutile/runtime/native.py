@@ -44,17 +44,24 @@ class Field(ctypes.Structure):
                 ("shape", ctypes.c_int64 * 3), ("strides", ctypes.c_int64 * 3)]
 
 
+MAX_FIELDS = 8
+MAX_SCALARS = 8
+
+
 class LaunchOpts(ctypes.Structure):
     _fields_ = [("halo", ctypes.c_int * 3), ("zchunk", ctypes.c_int), ("grid", ctypes.c_int),
                 ("loader", ctypes.c_int), ("bc_value", ctypes.c_double),
-                ("timeout_ns", ctypes.c_uint64)]
+                ("timeout_ns", ctypes.c_uint64), ("scalars", ctypes.c_double * MAX_SCALARS),
+                ("dyn", ctypes.c_void_p), ("red", ctypes.c_void_p),
+                ("bc_odd", ctypes.c_int * MAX_FIELDS)]
 
 
 class KernelDesc(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint if n == "magic" else ctypes.c_int) for n in (
         "magic", "ndim", "nin", "nout", "dtype_bytes", "rz", "ry", "rx", "rows", "tile_y",
         "tile_x", "vec", "threads", "stages", "nslot", "halo_chunks", "pad_left", "box_w",
-        "box_h", "smem_bytes", "zchunk", "temporal", "bc_mode", "min_blocks", "align")]
+        "box_h", "smem_bytes", "zchunk", "temporal", "bc_mode", "min_blocks", "align",
+        "nscalars", "ndyn", "reduce_max")]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -95,6 +102,13 @@ def library() -> ctypes.CDLL:
         lib.csd_apply_boundary.argtypes = [ctypes.POINTER(Field), ctypes.POINTER(ctypes.c_int),
                                            ctypes.c_int, ctypes.c_double, P]
         lib.csd_error_word.argtypes = [ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+        lib.csd_grid_size.restype = ctypes.c_size_t
+        lib.csd_cfl_update.argtypes = [ctypes.c_int, P, P, ctypes.c_double, ctypes.c_double, P, P]
+        lib.csd_grid_build.argtypes = [P, ctypes.POINTER(Field), ctypes.c_int, ctypes.POINTER(Field),
+                                       ctypes.c_int, ctypes.POINTER(LaunchOpts), P,
+                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        lib.csd_launch_batch.argtypes = [P, P, P, ctypes.c_int, ctypes.c_int,
+                                         ctypes.POINTER(LaunchOpts), P]
         lib.csd_reduce.argtypes = [ctypes.POINTER(Field), ctypes.POINTER(Field),
                                    ctypes.POINTER(ctypes.c_int), ctypes.c_int, P, ctypes.c_int, P,
                                    P]
@@ -220,11 +234,8 @@ def stream_handle(stream) -> int | None:
     return getattr(stream, "cuda_stream", None) or getattr(stream, "ptr", None)
 
 
-def launch(kernel: NativeKernel, inputs, outputs, halo, stream=None, *, zchunk: int = 0,
-           grid: int = 0, loader: int = -1, bc_value: float = 0.0, timeout_ns: int = 0) -> None:
-    lib = library()
-    fin = (Field * len(inputs))(*[field_of(t) for t in inputs])
-    fout = (Field * len(outputs))(*[field_of(t) for t in outputs])
+def make_opts(halo, *, zchunk: int = 0, grid: int = 0, loader: int = -1, bc_value: float = 0.0,
+              timeout_ns: int = 0, scalars=(), dyn=None, red=None, bc_odd=()) -> LaunchOpts:
     o = LaunchOpts()
     for i, h in enumerate(halo):
         o.halo[i] = int(h)
@@ -233,8 +244,56 @@ def launch(kernel: NativeKernel, inputs, outputs, halo, stream=None, *, zchunk: 
     o.loader = loader
     o.bc_value = bc_value
     o.timeout_ns = timeout_ns
+    if len(scalars) > MAX_SCALARS:
+        raise ValueError(f"at most {MAX_SCALARS} scalar parameters")
+    for i, v in enumerate(scalars):
+        o.scalars[i] = float(v)
+    o.dyn = None if dyn is None else (dyn if isinstance(dyn, int) else dyn.data_ptr())
+    o.red = None if red is None else (red if isinstance(red, int) else red.data_ptr())
+    for i, m in enumerate(bc_odd):
+        o.bc_odd[i] = int(m)
+    return o
+
+
+def launch(kernel: NativeKernel, inputs, outputs, halo, stream=None, **kw) -> None:
+    lib = library()
+    fin = (Field * len(inputs))(*[field_of(t) for t in inputs])
+    fout = (Field * len(outputs))(*[field_of(t) for t in outputs])
+    o = make_opts(halo, **kw)
     check(lib.csd_launch(kernel.handle, fin, len(inputs), fout, len(outputs), ctypes.byref(o),
                          ctypes.c_void_p(stream_handle(stream))))
+
+
+def grid_size() -> int:
+    return int(library().csd_grid_size())
+
+
+def grid_build(kernel: NativeKernel, inputs, outputs, halo, dest, **kw) -> tuple[int, int]:
+    """Write the descriptor of one batched grid into host buffer ``dest``
+    (a ctypes buffer of ``grid_size()`` bytes); returns (work items, loader)."""
+    lib = library()
+    fin = (Field * len(inputs))(*[field_of(t) for t in inputs])
+    fout = (Field * max(1, len(outputs)))(*[field_of(t) for t in outputs])
+    o = make_opts(halo, **kw)
+    items = ctypes.c_int()
+    loader = ctypes.c_int()
+    check(lib.csd_grid_build(kernel.handle, fin, len(inputs), fout, len(outputs), ctypes.byref(o),
+                             ctypes.cast(dest, ctypes.c_void_p), ctypes.byref(items),
+                             ctypes.byref(loader)))
+    return items.value, loader.value
+
+
+def launch_batch(kernel: NativeKernel, grids_ptr: int, item_start_ptr: int, ngrids: int,
+                 total_items: int, stream=None, grid: int = 0, timeout_ns: int = 0,
+                 loader: int = 0) -> None:
+    lib = library()
+    o = LaunchOpts()
+    o.grid = grid
+    o.loader = loader
+    o.timeout_ns = timeout_ns
+    check(lib.csd_launch_batch(kernel.handle, ctypes.c_void_p(grids_ptr),
+                               ctypes.c_void_p(item_start_ptr), ngrids, total_items,
+                               ctypes.byref(o), ctypes.c_void_p(stream_handle(stream))))
 
 
 def apply_boundary(t, halo, bc: str, value: float = 0.0, stream=None) -> None:
@@ -245,6 +304,14 @@ def apply_boundary(t, halo, bc: str, value: float = 0.0, stream=None) -> None:
                                  ctypes.c_void_p(stream_handle(stream))))
 
 
+def cfl_update(smax, scale, cfl: float, dt, dt_max: float = 1e30, stream=None) -> None:
+    """dt = min(cfl * scale / smax, dt_max) per grid, then smax = 0 (device arrays)."""
+    check(library().csd_cfl_update(int(smax.numel()), ctypes.c_void_p(smax.data_ptr()),
+                                   ctypes.c_void_p(scale.data_ptr()), float(cfl), float(dt_max),
+                                   ctypes.c_void_p(dt.data_ptr()),
+                                   ctypes.c_void_p(stream_handle(stream))))
+
+
 def error_word(reset: bool = True) -> int:
     v = ctypes.c_int()
     check(library().csd_error_word(ctypes.byref(v), 1 if reset else 0))
@@ -253,4 +320,5 @@ def error_word(reset: bool = True) -> int:
 
 __all__ = ["library", "check", "compile_source", "NativeModule", "NativeKernel", "launch",
            "apply_boundary", "error_word", "CsdError", "field_of", "default_cache_dir",
+           "make_opts", "grid_size", "grid_build", "launch_batch",
            "CSD_LOADER_TMA", "CSD_LOADER_LDG", "BC_MODES"]

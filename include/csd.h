@@ -50,18 +50,25 @@ typedef struct csd_field {
   int64_t strides[3];   /* elements; must describe a C-contiguous layout */
 } csd_field;
 
-/* Per-launch options (zero-initialise for defaults). */
+/* Per-launch (per-grid) options (zero-initialise for defaults). */
 typedef struct csd_launch_opts {
   int halo[3];          /* array halo width per array dim (interior = shape - 2*halo) */
-  int zchunk;           /* output rows per work item along dim 0 (0 = kernel default) */
+  int zchunk;           /* output rows per work item along dim 0 (0 = sized at launch) */
   int grid;             /* persistent CTAs (0 = occupancy x SM count) */
   int loader;           /* -1 auto, CSD_LOADER_TMA, CSD_LOADER_LDG */
   double bc_value;      /* Dirichlet value when the kernel fuses a boundary fill */
   uint64_t timeout_ns;  /* bound on device waits (0 = 2 s) */
+  double scalars[CSD_MAX_SCALARS];  /* values of the stencil's scalar parameters */
+  const double* dyn;    /* device array of per-grid dynamic scalars (e.g. dt), or NULL */
+  double* red;          /* device double receiving a max-reduction, or NULL */
+  int bc_odd[CSD_MAX_FIELDS];       /* per field: bit d = sign flip when mirrored in dim d */
 } csd_launch_opts;
 
 /* Library version (major*100 + minor). */
 int csd_version(void);
+
+/* sizeof(csd_grid), for callers that allocate descriptor arrays. */
+size_t csd_grid_size(void);
 
 /* Message of the last error on this thread ("" if none). */
 const char* csd_last_error(void);
@@ -103,6 +110,33 @@ int csd_kernel_resources(csd_kernel* k, int* regs, int* local_bytes, int* blocks
  * kernels, output halos untouched. */
 int csd_launch(csd_kernel* k, const csd_field* in, int n_in, const csd_field* out, int n_out,
                const csd_launch_opts* opts, void* stream);
+
+/* Describe one grid of a batched launch: validates the fields like
+ * csd_launch and writes the kernel-side descriptor (TMA maps included) into
+ * host memory `*g`; `*items` receives its number of work items and
+ * `*loader_used` the copy path it qualifies for (opts->loader = -1: TMA when
+ * aligned, else cp.async; all grids of one batch must use the same path).
+ * The caller copies the descriptors of all grids to device memory for
+ * csd_launch_batch.  No reference counterpart (the reference launches one
+ * grid per call). */
+int csd_grid_build(csd_kernel* k, const csd_field* in, int n_in, const csd_field* out, int n_out,
+                   const csd_launch_opts* opts, csd_grid* g, int* items, int* loader_used);
+
+/* One persistent launch over many grids of uneven sizes: `grids` (device)
+ * holds `ngrids` descriptors from csd_grid_build, `item_start` (device) the
+ * prefix sums of their work items (ngrids + 1 ints, last = total).  Work
+ * items are spread over the resident CTAs; each grid is advanced exactly as
+ * csd_launch would.  `grid` in `opts` overrides the CTA count; `loader` in
+ * `opts` selects the copy path the descriptors were built for. */
+int csd_launch_batch(csd_kernel* k, const csd_grid* grids, const int* item_start, int ngrids,
+                     int total_items, const csd_launch_opts* opts, void* stream);
+
+/* Per-grid CFL step for batched solvers (device arrays of length n):
+ * dt[i] = min(cfl * scale[i] / smax[i], dt_max) (dt_max when smax[i] is 0),
+ * then smax[i] = 0 for the next max-reduction.  No reference counterpart
+ * (the reference's examples use a fixed host-side dt). */
+int csd_cfl_update(int n, double* smax, const double* scale, double cfl, double dt_max,
+                   double* dt, void* stream);
 
 /* Fill the halo of `f` in place with boundary condition `bc` (CSD_BC_*),
  * dimension by dimension.  Equivalent of `apply_boundary_<name>(u)`

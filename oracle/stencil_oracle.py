@@ -336,3 +336,139 @@ def fused_kahan_step(inputs_by_name: dict, comps: dict, incr_fns: dict, ndim: in
         c_new[inner] = c2
         out[name] = (u_new, c_new)
     return out
+
+
+# --------------------------------------------------------------------------- #
+# Runge-Kutta stages with FP64 combination, CFL steps (batched solvers)
+# --------------------------------------------------------------------------- #
+
+
+def evaluate_ops(arrays_by_param: dict, fn, ndim: int, halo, shape, dtype, scalars=None):
+    """Like ``evaluate`` but scalar parameters are bound from ``scalars`` and a
+    tuple-returning body gives a tuple."""
+    import inspect
+
+    f = raw_fn(fn)
+    params = list(inspect.signature(f).parameters)[:-ndim]
+    scalars = scalars or {}
+    args = []
+    for p in params:
+        if p in scalars:
+            args.append(float(scalars[p]))
+        else:
+            args.append(ArrayProxy(arrays_by_param.get(p, np.zeros(shape, dtype)), halo))
+    res = array_aware(f)(*args, *([0] * ndim))
+    return res if isinstance(res, tuple) else (res,)
+
+
+def reflect_fill(u: np.ndarray, halo, odd_dims=()) -> None:
+    """Reflecting walls with the sign of mirrored values flipped in ``odd_dims``
+    (a wall's normal momentum); corners take the product of the signs."""
+    apply_boundary(u, uniform_spec("reflecting", u.ndim), halo)
+    for d in odd_dims:
+        sl = [slice(None)] * u.ndim
+        sl[d] = slice(0, halo[d])
+        u[tuple(sl)] *= -1
+        sl[d] = slice(u.shape[d] - halo[d], u.shape[d])
+        u[tuple(sl)] *= -1
+
+
+def rk_stage(op, names, stage, base, acc, coeffs, dt: float, ndim: int, halo, scalars=None,
+             boundary=None, odd=None):
+    """One fused RK stage as the stage kernels compute it.
+
+    ``stage``/``base``/``acc``: tuples of state arrays (base/acc may be None);
+    ``coeffs = (a, b, c, w)``.  The stage state is boundary-filled (copies)
+    first when ``boundary`` is ``"reflecting"`` (``odd[m]``: dims whose mirror
+    flips field m's sign).  Returns (next, acc_next) tuples, interiors only
+    meaningful; the combination is FP64 in the kernels' order with one
+    rounding to the field dtype.
+    """
+    a, b, c, w = coeffs
+    filled = []
+    for m, s in enumerate(stage):
+        t = s.copy()
+        if boundary == "reflecting":
+            reflect_fill(t, halo, (odd or {}).get(m, ()))
+        elif boundary is not None:
+            apply_boundary(t, uniform_spec(boundary, ndim), halo)
+        filled.append(t)
+    dt_ = stage[0].dtype
+    L = evaluate_ops(dict(zip(names, filled)), op, ndim, halo, stage[0].shape, dt_, scalars)
+    inner = _interior(stage[0].shape, halo)
+    nxt, accn = [], []
+    cdt = c * dt
+    for m, lm in enumerate(L):
+        lm64 = np.asarray(lm, dtype=np.float64)
+        x = None
+        if a != 0.0:
+            bb = base[m][inner].astype(np.float64)
+            x = bb if a == 1.0 else a * bb
+        if b != 0.0:
+            sv = stage[m][inner].astype(np.float64)
+            y = sv if b == 1.0 else b * sv
+            x = y if x is None else x + y
+        term = cdt * lm64
+        x = term if x is None else x + term
+        out = np.zeros_like(stage[m])
+        out[inner] = x.astype(dt_)
+        nxt.append(out)
+        if w is not None:
+            ao = np.zeros_like(stage[m])
+            ao[inner] = (acc[m][inner].astype(np.float64) + (w * dt) * lm64).astype(dt_)
+            accn.append(ao)
+    return tuple(nxt), tuple(accn)
+
+
+RK_TABLES = {
+    "euler": [(1.0, 0.0, 1.0, None, "u", "u", None, "s1")],
+    "rk2": [(1.0, 0.0, 0.5, None, "u", "u", None, "s1"),
+            (1.0, 0.0, 1.0, None, "u", "s1", None, "u")],
+    "rk4": [(1.0, 0.0, 0.5, 1.0 / 6.0, "u", "u", "u", "s1"),
+            (1.0, 0.0, 0.5, 1.0 / 3.0, "u", "s1", "acc", "s2"),
+            (1.0, 0.0, 1.0, 1.0 / 3.0, "u", "s2", "acc", "s3"),
+            (1.0, 0.0, 1.0 / 6.0, None, "acc", "s3", None, "u")],
+    "ssprk3": [(1.0, 0.0, 1.0, None, "u", "u", None, "s1"),
+               (0.75, 0.25, 0.25, None, "u", "s1", None, "s2"),
+               (1.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0, None, "u", "s2", None, "u")],
+}
+
+
+def rk_step(op, names, state, method: str, dt: float, ndim: int, halo, scalars=None,
+            boundary=None, odd=None):
+    """One RK step (the fused-stage formulation); returns the new state tuple."""
+    bufs = {"u": tuple(state)}
+    for a, b, c, w, base, stage, acc_in, out in RK_TABLES[method]:
+        nxt, accn = rk_stage(op, names, bufs[stage], bufs[base] if a != 0.0 else None,
+                             bufs[acc_in] if w is not None else None, (a, b, c, w), dt, ndim,
+                             halo, scalars, boundary, odd)
+        inner = _interior(state[0].shape, halo)
+        if out == "u":
+            new = []
+            for old, n in zip(bufs["u"], nxt):
+                t = old.copy()
+                t[inner] = n[inner]
+                new.append(t)
+            bufs["u"] = tuple(new)
+        else:
+            bufs[out] = nxt
+        if w is not None:
+            bufs["acc"] = accn
+    if RK_TABLES[method][-1][7] != "u":
+        last = bufs[RK_TABLES[method][-1][7]]
+        new = []
+        for old, n in zip(state, last):
+            t = old.copy()
+            inner = _interior(old.shape, halo)
+            t[inner] = n[inner]
+            new.append(t)
+        bufs["u"] = tuple(new)
+    return bufs["u"]
+
+
+def cfl_dt(speed_fn, state, names, ndim, halo, cfl: float, scale: float) -> float:
+    """dt = cfl * scale / max(signal speed over the interior)."""
+    (sp,) = evaluate_ops(dict(zip(names, state)), speed_fn, ndim, halo, state[0].shape,
+                         state[0].dtype)
+    smax = float(np.max(np.asarray(sp, dtype=np.float64)))
+    return (cfl * scale) / smax

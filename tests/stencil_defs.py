@@ -142,3 +142,66 @@ def gray_scott_init(n: int, seed: int = 2, halo=(1, 1), dtype="float64"):
         u[sl] = 0.5 * (1 + rng.uniform(-0.01, 0.01, (32, 32)))
         v[sl] = 0.25 * (1 + rng.uniform(-0.01, 0.01, (32, 32)))
     return u.astype(dtype), v.astype(dtype)
+
+
+# Nonlinear shallow water (h, hu, hv) on a square grid, x = j (columns),
+# y = i (rows): the right-hand side with local Lax-Friedrichs (Rusanov) fluxes
+# and the signal speed for the CFL step.  `sqrt` comes from the executor.
+G_SW = 9.81
+
+
+def sw_rhs(h, hu, hv, dx, i, j):
+    hC = h[i, j]; huC = hu[i, j]; hvC = hv[i, j]
+    hE = h[i, j + 1]; huE = hu[i, j + 1]; hvE = hv[i, j + 1]
+    hW = h[i, j - 1]; huW = hu[i, j - 1]; hvW = hv[i, j - 1]
+    hN = h[i + 1, j]; huN = hu[i + 1, j]; hvN = hv[i + 1, j]
+    hS = h[i - 1, j]; huS = hu[i - 1, j]; hvS = hv[i - 1, j]
+    uC = huC / hC; vC = hvC / hC; cC = sqrt(G_SW * hC)  # noqa: F821
+    uE = huE / hE; cE = sqrt(G_SW * hE)  # noqa: F821
+    uW = huW / hW; cW = sqrt(G_SW * hW)  # noqa: F821
+    vN = hvN / hN; cN = sqrt(G_SW * hN)  # noqa: F821
+    vS = hvS / hS; cS = sqrt(G_SW * hS)  # noqa: F821
+    pC = 0.5 * G_SW * hC * hC
+    fuC = huC * uC + pC; fvC = huC * vC
+    fuE = huE * uE + 0.5 * G_SW * hE * hE; fvE = hvE * uE
+    fuW = huW * uW + 0.5 * G_SW * hW * hW; fvW = hvW * uW
+    guC = hvC * uC; gvC = hvC * vC + pC
+    guN = huN * vN; gvN = hvN * vN + 0.5 * G_SW * hN * hN
+    guS = huS * vS; gvS = hvS * vS + 0.5 * G_SW * hS * hS
+    aE = max(abs(uC) + cC, abs(uE) + cE)
+    aW = max(abs(uW) + cW, abs(uC) + cC)
+    bN = max(abs(vC) + cC, abs(vN) + cN)
+    bS = max(abs(vS) + cS, abs(vC) + cC)
+    FhE = 0.5 * (huC + huE) - 0.5 * aE * (hE - hC)
+    FhW = 0.5 * (huW + huC) - 0.5 * aW * (hC - hW)
+    FuE = 0.5 * (fuC + fuE) - 0.5 * aE * (huE - huC)
+    FuW = 0.5 * (fuW + fuC) - 0.5 * aW * (huC - huW)
+    FvE = 0.5 * (fvC + fvE) - 0.5 * aE * (hvE - hvC)
+    FvW = 0.5 * (fvW + fvC) - 0.5 * aW * (hvC - hvW)
+    GhN = 0.5 * (hvC + hvN) - 0.5 * bN * (hN - hC)
+    GhS = 0.5 * (hvS + hvC) - 0.5 * bS * (hC - hS)
+    GuN = 0.5 * (guC + guN) - 0.5 * bN * (huN - huC)
+    GuS = 0.5 * (guS + guC) - 0.5 * bS * (huC - huS)
+    GvN = 0.5 * (gvC + gvN) - 0.5 * bN * (hvN - hvC)
+    GvS = 0.5 * (gvS + gvC) - 0.5 * bS * (hvC - hvS)
+    return (-(FhE - FhW) / dx - (GhN - GhS) / dx,
+            -(FuE - FuW) / dx - (GuN - GuS) / dx,
+            -(FvE - FvW) / dx - (GvN - GvS) / dx)
+
+
+def sw_speed(h, hu, hv, i, j):
+    return max(abs(hu[i, j] / h[i, j]), abs(hv[i, j] / h[i, j])) + sqrt(G_SW * h[i, j])  # noqa: F821
+
+
+def sw_init(n: int, rng, halo=(1, 1), dtype="float32"):
+    """h = 1 + 0.1 * Gaussian bump at a random centre, hu = hv = 0."""
+    import numpy as np
+
+    y = (np.arange(n) + 0.5) / n
+    cy, cx = rng.uniform(0.2, 0.8, size=2)
+    r2 = (y[:, None] - cy) ** 2 + (y[None, :] - cx) ** 2
+    shape = (n + 2 * halo[0], n + 2 * halo[1])
+    h = np.ones(shape)
+    h[halo[0]:halo[0] + n, halo[1]:halo[1] + n] = 1.0 + 0.1 * np.exp(-r2 / (2 * 0.05 ** 2))
+    z = np.zeros(shape)
+    return h.astype(dtype), z.astype(dtype), z.astype(dtype)
