@@ -332,6 +332,317 @@ def run_reference(args) -> dict | None:
     }
 
 
+# ---------------------------------------------------------------------------
+# Batched shallow water: 256 independent 2-D grids, RK2, CFL 0.4, reflective
+# ---------------------------------------------------------------------------
+SW_GRIDS = 256
+SW_STEPS = 200
+SW_METRIC = "solves/s (256 batched 2-D shallow-water RK2 solves, 200 steps each)"
+SW_BC_ODD = (0, 2, 1)   # hu flips sign across x walls (dim 1), hv across y walls (dim 0)
+
+
+SW_FIXED_N = 0          # > 0: every grid n x n (small profiling cases)
+SW_ZCHUNK = 0           # > 0: rows per batched work item (0: the kernels' default)
+
+
+def _sw_workload(seed: int = 3):
+    """Sizes log-uniform in [64, 2048] and the h-bump initial states (seeded)."""
+    import numpy as np
+
+    import stencil_defs as D
+
+    rng = np.random.default_rng(seed)
+    sizes = [int(x) for x in np.rint(np.exp(rng.uniform(np.log(64), np.log(2048), SW_GRIDS)))]
+    if SW_FIXED_N > 0:
+        sizes = [SW_FIXED_N] * SW_GRIDS
+    init = [D.sw_init(N, rng, halo=(1, 1), dtype="float64") for N in sizes]
+    return sizes, init
+
+
+def _sw_programs(dtype: str):
+    import stencil_defs as D
+    from cutile import RKIntegrator, stencil
+    from cutile import compile as stencil_compile
+
+    rk = RKIntegrator(stencil(ndim=2, dtype=dtype)(D.sw_rhs), "rk2").compile(
+        boundary="reflecting", align_halo=False)
+    speed = stencil_compile(stencil(ndim=2, dtype=dtype)(D.sw_speed), reduce="max",
+                            align_halo=False)
+    return rk, speed
+
+
+def _sw_batch(dtype: str, sizes, init, device):
+    """Row-pitched packed fields, an RKBatch with per-grid CFL dt, and a
+    device copy of the initial state for resets."""
+    import numpy as np
+    import torch
+
+    from cutile.runtime.rk_runtime import RKBatch, pack_grids
+
+    rk, speed = _sw_programs(dtype)
+    tdt = torch.float64 if dtype == "float64" else torch.float32
+    flat, states = pack_grids([a[0].shape for a in init], 3, tdt, device)
+    for st, fields in zip(states, init):
+        for dst, src in zip(st, fields):
+            dst.copy_(torch.from_numpy(np.ascontiguousarray(src, dtype=np.dtype(dtype))))
+    dx = [1.0 / N for N in sizes]
+    batch = RKBatch(rk, states, [{"dx": d} for d in dx],
+                    cfl=(speed.load_module().program(), dx, 0.4), bc_odd=SW_BC_ODD,
+                    zchunk=SW_ZCHUNK or None)
+    return batch, flat, flat.clone(), states, (rk, speed)
+
+
+def _sw_cpu_job(args):
+    """One worker: oracle RK2 + CFL steps of one seeded grid; returns
+    (seconds, point-steps)."""
+    n, steps, seed = args
+    import numpy as np
+
+    import stencil_defs as D
+    from oracle import stencil_oracle as O
+
+    rng = np.random.default_rng(seed)
+    st = tuple(a.astype(np.float32) for a in D.sw_init(n, rng, halo=(1, 1), dtype="float64"))
+    names = ["h", "hu", "hv"]
+    odd = {1: (1,), 2: (0,)}
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        dt = O.cfl_dt(D.sw_speed, st, names, 2, (1, 1), 0.4, 1.0 / n)
+        st = O.rk_step(D.sw_rhs, names, st, "rk2", dt, 2, (1, 1), {"dx": 1.0 / n},
+                       "reflecting", odd)
+    return time.perf_counter() - t0, n * n * steps
+
+
+def sw_cpu_baseline(total_point_steps: float, cores: int, n: int = 256, steps: int = 4) -> dict:
+    """The oracle (NumPy restatement of the reference's RK stepping around
+    apply_stencil) on ``cores`` worker processes, each a seeded n^2 grid;
+    solves/s extrapolated from the measured point-steps/s."""
+    import multiprocessing as mp
+
+    if cores == 1:
+        secs, pts = _sw_cpu_job((n, steps, 0))
+        rate, wall = pts / secs, secs
+    else:
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(cores) as pool:
+            pool.map(_sw_cpu_job, [(64, 1, k) for k in range(cores)])
+            t0 = time.perf_counter()
+            res = pool.map(_sw_cpu_job, [(n, steps, k) for k in range(cores)])
+            wall = time.perf_counter() - t0
+        rate = sum(p for _, p in res) / wall
+    solves = SW_GRIDS * rate / total_point_steps
+    return {"value": solves, "unit": "solves/s", "cores": cores, "kind": "port",
+            "sample": f"{cores} x {steps} RK2+CFL steps of a {n}^2 float32 grid (oracle rk_step, "
+                      f"wall {wall:.1f} s), {rate / 1e6:.2f} M point-steps/s extrapolated to the "
+                      f"workload's {total_point_steps:.3g} point-steps"}
+
+
+def run_sw_batch(args) -> dict | None:
+    import numpy as np
+    import torch
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        torch.distributed.init_process_group("nccl", init_method="env://")
+    sizes, init = _sw_workload(seed=3 + rank)
+    pts = sum(N * N for N in sizes)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def timed(fn, steps):
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        ev0.record(stream)
+        for _ in range(steps):
+            fn()
+        ev1.record(stream)
+        barrier()
+        ms = ev0.elapsed_time(ev1)
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms / steps
+
+    runs = {}
+    for dtype in (("float32", "float64") if args.compare else ("float32",)):
+        batch, flat, flat0, states, _ = _sw_batch(dtype, sizes, init, dev)
+        graph = batch.capture(SW_STEPS)
+
+        def solve_set(flat=flat, flat0=flat0, graph=graph):
+            flat.copy_(flat0)
+            graph.replay()
+
+        for _ in range(args.warmup):
+            solve_set()
+        torch.cuda.synchronize()
+        if dtype == "float32":
+            with ClockSampler(local) as clk:
+                ms = timed(solve_set, args.steps)
+            clocks = clk.summary()
+        else:
+            ms = timed(solve_set, max(1, args.steps // 2))
+        solve_set()
+        torch.cuda.synchronize()
+        runs[dtype] = {"ms": ms, "batch": batch, "flat": flat, "flat0": flat0, "graph": graph,
+                       "states": states}
+
+    if not args.compare:
+        ms32 = runs["float32"]["ms"]
+        return {"metric": SW_METRIC, "value": round(SW_GRIDS * world / (ms32 / 1e3), 3),
+                "unit": "solves/s", "ms_per_step": round(ms32, 3), "n_gpus": world,
+                "config": {"workload": f"{SW_GRIDS} grids, fixed n={SW_FIXED_N}, "
+                                       f"{SW_STEPS} RK2 steps (profiling case, no comparison)"},
+                "gpu_launches": (1 + SW_STEPS * runs["float32"]["batch"].launches_per_step())
+                * args.steps} if rank == 0 else None
+    # relative L2 of the FP32 solves against the FP64 solves, per field, worst grid
+    rel = [0.0, 0.0, 0.0]
+    for a, b in zip(runs["float32"]["states"], runs["float64"]["states"]):
+        for f in range(3):
+            ia, ib = a[f][1:-1, 1:-1].double(), b[f][1:-1, 1:-1]
+            nb = float(torch.linalg.norm(ib))
+            if nb > 0:
+                rel[f] = max(rel[f], float(torch.linalg.norm(ia - ib)) / nb)
+    ms64 = runs.pop("float64")["ms"]
+    torch.cuda.empty_cache()
+
+    # the plain FP64 path: every grid on its own through the drop-in API
+    # (one reduction, one dt update and one launch per RK stage, per grid,
+    # eagerly), timed on a bounded number of steps and scaled to 200
+    rk64, speed64 = _sw_programs("float64")
+    prog = rk64.load_module().program()
+    prog.bc_odd = SW_BC_ODD
+    sp = speed64.load_module().program()
+    st64 = [tuple(torch.from_numpy(a).to(dev) for a in g) for g in init]
+    n = len(st64)
+    smax = torch.zeros(n, dtype=torch.float64, device=dev)
+    dts = torch.zeros(n, dtype=torch.float64, device=dev)
+    scale = torch.tensor([1.0 / N for N in sizes], dtype=torch.float64, device=dev)
+    from cutile.runtime import native
+
+    def plain_step():
+        for g, st in enumerate(st64):
+            sp.reduce(list(st), out=smax[g])
+            native.cfl_update(smax[g:g + 1], scale[g:g + 1], 0.4, dts[g:g + 1], 1e30, stream)
+            prog.step(st, dts[g:g + 1], scalars={"dx": 1.0 / sizes[g]})
+
+    plain_steps = 10
+    plain_step()
+    torch.cuda.synchronize()
+    plain_ms = timed(plain_step, plain_steps) * SW_STEPS
+    plain_launches = n * (2 + len(prog.table))
+
+    ms32 = runs["float32"]["ms"]
+    value = SW_GRIDS * world / (ms32 / 1e3)
+    b32 = runs["float32"]["batch"]
+    launches = 1 + SW_STEPS * b32.launches_per_step()
+
+    # roofline of the FP32 batched step: algorithmic bytes per RK2 step =
+    # 15 field transfers (stage 1: 3 in + 3 out; stage 2: 6 in + 3 out) plus
+    # the CFL reduction's 3 reads, 4 B each, per interior point
+    alg_bytes = 18 * 4 * pts
+    step_ms = ms32 / SW_STEPS
+    achieved = alg_bytes / (step_ms / 1e3) / 1e9
+    peak, peak_kind = _peaks()
+
+    # end-to-end: pinned host state -> device, 200 graph steps, result -> host
+    flat, graph = runs["float32"]["flat"], runs["float32"]["graph"]
+    host_in = runs["float32"]["flat0"].cpu().pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+
+    def e2e_set():
+        flat.copy_(host_in, non_blocking=True)
+        graph.replay()
+        host_out.copy_(flat, non_blocking=True)
+
+    e2e_set()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_ms = timed(e2e_set, 2)
+    e2e_ms = max(e2e_ms, (time.perf_counter() - t0) * 1e3 / 2)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = sw_cpu_baseline(float(pts) * SW_STEPS, os.cpu_count() or 1)
+    line = {
+        "metric": SW_METRIC, "value": round(value, 3), "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms32, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (FP64 RK combination)", "data": "synthetic",
+        "config": {"workload": "256 shallow-water grids (h, hu, hv; Rusanov fluxes; g=9.81), N "
+                               "log-uniform in [64, 2048] (seed 3), h = 1 + 0.1 Gaussian bump, "
+                               "RK2 with FP64 stage combination, CFL 0.4 per grid on the device, "
+                               "reflective walls fused into staging; one step = reset from the "
+                               "resident initial state + 200 RK2 steps replayed from one CUDA "
+                               "graph (one persistent launch per stage over all grids)",
+                   "grids": SW_GRIDS, "interior_points": pts, "rk_steps": SW_STEPS,
+                   "l2": f"fields {flat.numel() * 4 / 1e9:.2f} GB >> 126 MB L2, no flush",
+                   "parallelism": f"replicas{world}"},
+        "comparison": {
+            "fp64_batched_solves_s": round(SW_GRIDS * world / (ms64 / 1e3), 3),
+            "fp64_plain_solves_s": round(SW_GRIDS * world / (plain_ms / 1e3), 3),
+            "speedup_vs_fp64_plain": round(plain_ms / ms32, 3),
+            "speedup_vs_fp64_batched": round(ms64 / ms32, 3),
+            "fp64_plain": f"per grid and step: reduce + dt update + {len(prog.table)} stage "
+                          f"launches through the drop-in API ({plain_launches} launches per "
+                          f"step), eager; timed over {plain_steps} steps, scaled to "
+                          f"{SW_STEPS}",
+            "rel_l2_fp32_vs_fp64": {"h": rel[0], "hu": rel[1], "hv": rel[2],
+                                    "over": "interiors after 200 steps, worst grid"},
+        },
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                     "peak_kind": peak_kind, "kernel": "whole RK2 step (4 launches)",
+                     "algorithmic_bytes_per_step": alg_bytes},
+        "e2e": {"value": round(SW_GRIDS * world / (e2e_ms / 1e3), 3), "unit": "solves/s",
+                "h2d_bytes_per_step": int(host_in.numel() * 4),
+                "d2h_bytes_per_step": int(host_out.numel() * 4),
+                "step": "H2D of all fields, 200-step graph replay, D2H of all fields"},
+        "gpu_launches": launches * args.steps,
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    del runs
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return line if rank == 0 else None
+
+
+def run_sw_reference(args) -> dict | None:
+    world, rank, _ = _dist()
+    if rank != 0:
+        return None
+    sizes, _ = _sw_workload()
+    pts = float(sum(N * N for N in sizes)) * SW_STEPS
+    cores = os.cpu_count() or 1
+    vals = []
+    for k in range(args.warmup + args.steps):
+        cb = sw_cpu_baseline(pts, cores, n=128, steps=2)
+        if k >= args.warmup:
+            vals.append(cb["value"])
+    value = statistics.median(vals)
+    cb["value"] = value
+    return {
+        "metric": SW_METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(SW_GRIDS / value * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic", "impl": "reference",
+        "config": {"workload": f"256 shallow-water grids, RK2 + CFL, CPU NumPy oracle on {cores} "
+                               f"processes, sampled grids extrapolated"},
+        "cpu_baseline": cb,
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -342,12 +653,28 @@ def main() -> None:
     ap.add_argument("--temporal", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--n", type=int, default=512, help="interior extent per dimension")
+    ap.add_argument("--workload", choices=("lap7", "sw_batch"), default="lap7",
+                    help="lap7: 3-D 7-point 512^3 sweeps; sw_batch: 256 batched shallow-water "
+                         "solves")
+    ap.add_argument("--sw-grids", type=int, default=256, help="sw_batch: number of grids")
+    ap.add_argument("--sw-n", type=int, default=0,
+                    help="sw_batch: fixed grid size (0 = log-uniform in [64, 2048])")
+    ap.add_argument("--sw-steps", type=int, default=200, help="sw_batch: RK2 steps per solve")
+    ap.add_argument("--sw-zchunk", type=int, default=0,
+                    help="sw_batch: rows per work item (0: the kernels' default)")
+    ap.add_argument("--no-compare", dest="compare", action="store_false",
+                    help="sw_batch: time the FP32 batch only (profiling cases)")
     args = ap.parse_args()
-    global N_INTERIOR
+    global N_INTERIOR, SW_GRIDS, SW_FIXED_N, SW_STEPS, SW_ZCHUNK
     N_INTERIOR = args.n
+    SW_GRIDS, SW_FIXED_N, SW_STEPS = args.sw_grids, args.sw_n, args.sw_steps
+    SW_ZCHUNK = args.sw_zchunk
     if args.warmup < 3:
         args.warmup = 3
-    line = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if args.workload == "sw_batch":
+        line = run_sw_reference(args) if args.impl == "reference" else run_sw_batch(args)
+    else:
+        line = run_reference(args) if args.impl == "reference" else run_ours(args)
     if line is not None:
         print(json.dumps(line), flush=True)
 

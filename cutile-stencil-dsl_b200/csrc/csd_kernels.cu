@@ -93,10 +93,21 @@ int apply_boundary_t(const csd_field* f, const int* halo, int bc, double value, 
 
 }  // namespace
 
+// The fill and reduction kernels index packed (C-contiguous) arrays.
+static bool packed(const csd_field* f) {
+  long long expect = 1;
+  for (int i = f->ndim - 1; i >= 0; --i) {
+    if (f->shape[i] != 1 && f->strides[i] != expect) return false;
+    expect *= f->shape[i];
+  }
+  return true;
+}
+
 extern "C" int csd_apply_boundary(const csd_field* f, const int* halo, int bc, double value,
                                   void* stream) {
   if (!f || !halo || !f->ptr) return csd_internal_fail(CSD_EINVAL, "null argument");
   if (f->ndim < 1 || f->ndim > 3) return csd_internal_fail(CSD_EINVAL, "ndim must be 1-3");
+  if (!packed(f)) return csd_internal_fail(CSD_EINVAL, "boundary fill needs a C-contiguous field");
   if (bc < CSD_BC_DIRICHLET || bc > CSD_BC_REFLECTING)
     return csd_internal_fail(CSD_EINVAL, "unknown boundary condition");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
@@ -214,10 +225,12 @@ extern "C" int csd_reduce(const csd_field* a, const csd_field* b, const int* hal
   if (!a || !a->ptr || !halo || !partials || !result || nblocks < 1)
     return csd_internal_fail(CSD_EINVAL, "null argument or nblocks < 1");
   if (a->ndim < 1 || a->ndim > 3) return csd_internal_fail(CSD_EINVAL, "ndim must be 1-3");
+  if (!packed(a)) return csd_internal_fail(CSD_EINVAL, "reductions need C-contiguous fields");
   const bool diff = (op == CSD_RED_DIFF_SUMSQ || op == CSD_RED_DIFF_MAXABS);
   if (diff) {
     if (!b || !b->ptr || b->dtype != a->dtype || b->ndim != a->ndim)
       return csd_internal_fail(CSD_EINVAL, "difference reductions need a second field like the first");
+    if (!packed(b)) return csd_internal_fail(CSD_EINVAL, "reductions need C-contiguous fields");
     for (int i = 0; i < a->ndim; ++i)
       if (b->shape[i] != a->shape[i]) return csd_internal_fail(CSD_EINVAL, "field shapes differ");
   }

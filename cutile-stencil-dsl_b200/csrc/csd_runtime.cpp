@@ -459,12 +459,12 @@ static void view3(const csd_field& f, long long dims[3], const int halo_in[3], i
   }
 }
 
-static bool contiguous(const csd_field& f) {
-  long long expect = 1;
-  for (int i = f.ndim - 1; i >= 0; --i) {
-    if (f.shape[i] != 1 && f.strides[i] != expect) return false;
-    expect *= f.shape[i];
-  }
+// Row-pitched layout: unit innermost stride, each outer stride spanning at
+// least the dimension inside it (C-contiguous arrays are the tight case).
+static bool row_pitched(const csd_field& f) {
+  if (f.shape[f.ndim - 1] != 1 && f.strides[f.ndim - 1] != 1) return false;
+  for (int i = f.ndim - 2; i >= 0; --i)
+    if (f.shape[i] != 1 && f.strides[i] < f.strides[i + 1] * f.shape[i + 1]) return false;
   return true;
 }
 
@@ -490,7 +490,10 @@ static int build_grid(csd_kernel* k, const csd_field* in, int n_in, const csd_fi
     for (int d = 0; d < f.ndim; ++d)
       if (f.shape[d] != f0.shape[d]) return fail(CSD_EINVAL, "all fields must have the same shape");
     if (f.dtype != want_dtype) return fail(CSD_EINVAL, "field dtype does not match the kernel");
-    if (!contiguous(f)) return fail(CSD_EINVAL, "fields must be C-contiguous");
+    if (!row_pitched(f)) return fail(CSD_EINVAL, "fields must be C-contiguous or row-pitched");
+    for (int d = 0; d < f.ndim; ++d)
+      if (f.shape[d] != 1 && f.strides[d] != f0.strides[d])
+        return fail(CSD_EINVAL, "all fields of a grid must have the same strides");
     if (!f.ptr) return fail(CSD_EINVAL, "null field pointer");
     if ((reinterpret_cast<uintptr_t>(f.ptr) % D.dtype_bytes) != 0)
       return fail(CSD_EALIGN, "field pointer not aligned to its element size");
@@ -512,8 +515,16 @@ static int build_grid(csd_kernel* k, const csd_field* in, int n_in, const csd_fi
     if (halo[d] < rad[d])
       return fail(CSD_EINVAL, "array halo %d is smaller than the stencil radius %d", halo[d], rad[d]);
   }
-  g->pitch_y = g->dims[2];
-  g->pitch_z = g->dims[1] * g->dims[2];
+  if (f0.ndim == 3) {
+    g->pitch_y = f0.shape[1] == 1 ? f0.shape[2] : f0.strides[1];
+    g->pitch_z = f0.shape[0] == 1 ? f0.shape[1] * g->pitch_y : f0.strides[0];
+  } else if (f0.ndim == 2) {
+    g->pitch_y = f0.shape[0] == 1 ? f0.shape[1] : f0.strides[0];
+    g->pitch_z = g->pitch_y;
+  } else {
+    g->pitch_y = g->dims[2];
+    g->pitch_z = g->dims[2];
+  }
   for (int i = 0; i < n_in; ++i) g->in[i] = in[i].ptr;
   for (int i = 0; i < n_out; ++i) g->out[i] = out[i].ptr;
   g->xbase = (g->halo[2] / D.align) * D.align;
@@ -521,7 +532,7 @@ static int build_grid(csd_kernel* k, const csd_field* in, int n_in, const csd_fi
   g->tiles[1] = (g->interior[1] + D.tile_y - 1) / D.tile_y;
   const long long esz = D.dtype_bytes;
   // Loader: TMA when every input is 16-byte aligned with 16-byte pitches.
-  bool tma_ok = ((g->dims[2] * esz) % 16 == 0) && ((g->pitch_z * esz) % 16 == 0);
+  bool tma_ok = ((g->pitch_y * esz) % 16 == 0) && ((g->pitch_z * esz) % 16 == 0);
   for (int i = 0; i < n_in; ++i) tma_ok = tma_ok && (reinterpret_cast<uintptr_t>(in[i].ptr) % 16 == 0);
   int loader = loader_req;
   if (loader < 0 || loader > 1) loader = tma_ok ? CSD_LOADER_TMA : CSD_LOADER_LDG;
@@ -535,7 +546,9 @@ static int build_grid(csd_kernel* k, const csd_field* in, int n_in, const csd_fi
   const long long columns = (long long)g->tiles[0] * g->tiles[1];
   int zchunk = o.zchunk > 0 ? o.zchunk : D.zchunk;
   if (zchunk <= 0) {
-    long long nzc = slots / (columns > 0 ? columns : 1);
+    // -W: W items per resident block (issue-bound bodies balance better)
+    const long long waves = zchunk < 0 ? -(long long)zchunk : 1;
+    long long nzc = slots * waves / (columns > 0 ? columns : 1);
     if (nzc < 1) nzc = 1;
     if (nzc > g->interior[0]) nzc = g->interior[0];
     zchunk = (int)((g->interior[0] + nzc - 1) / nzc);

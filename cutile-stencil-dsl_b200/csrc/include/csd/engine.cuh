@@ -180,6 +180,46 @@ __device__ __forceinline__ long long bc_map(long long i, int h, int n, int mode)
 }
 
 // ---------------------------------------------------------------------------
+// Correctly rounded division and square root for stencil bodies
+// ---------------------------------------------------------------------------
+// The IEEE-exact __fdiv_rn/__ddiv_rn/__fsqrt_rn/__dsqrt_rn sequences send a
+// zero dividend or radicand to their out-of-line fix-up path.  In a field at
+// rest (zero momenta, zero flux differences) that is the common case and
+// doubles a flux stencil's instruction count, so the zero cases are settled
+// here by their IEEE definitions and the intrinsic only sees non-zero
+// operands: 0/y is a zero signed sign(x) XOR sign(y) for y != 0 and y not NaN,
+// 0/0 and 0/NaN are NaN, sqrt(+-0) is +-0.  Every result equals the
+// intrinsic's own.
+__device__ __forceinline__ float div_rn(float x, float y) {
+  const bool z = (x == 0.0f);
+  const float q = __fdiv_rn(z ? 1.0f : x, y);
+  const float zq = (y == 0.0f || y != y)
+                       ? __int_as_float(0x7fffffff)
+                       : __int_as_float((__float_as_int(x) ^ __float_as_int(y)) & 0x80000000);
+  return z ? zq : q;
+}
+__device__ __forceinline__ double div_rn(double x, double y) {
+  const bool z = (x == 0.0);
+  const double q = __ddiv_rn(z ? 1.0 : x, y);
+  const double zq =
+      (y == 0.0 || y != y)
+          ? __longlong_as_double(0x7fffffffffffffffll)
+          : __longlong_as_double((__double_as_longlong(x) ^ __double_as_longlong(y)) &
+                                 (long long)0x8000000000000000ull);
+  return z ? zq : q;
+}
+__device__ __forceinline__ float sqrt_rn(float x) {
+  const bool z = (x == 0.0f);
+  const float r = __fsqrt_rn(z ? 1.0f : x);
+  return z ? x : r;
+}
+__device__ __forceinline__ double sqrt_rn(double x) {
+  const bool z = (x == 0.0);
+  const double r = __dsqrt_rn(z ? 1.0 : x);
+  return z ? x : r;
+}
+
+// ---------------------------------------------------------------------------
 // Chunk loaders
 // ---------------------------------------------------------------------------
 template <class C>
@@ -226,53 +266,74 @@ struct Loader {
 // interior with their boundary-condition values (fused boundary fill).
 // `bc_odd[f]` bit d: a value mirrored across a boundary of dim d changes
 // sign (a wall's normal momentum); the sign is the product over mirrored dims.
+// One warp per chunk line (Z row, Y row): lines outside the interior in Z or
+// Y are patched whole, the others only in their out-of-interior X ranges.
+template <class C>
+__device__ __forceinline__ void patch_cell(const csd_grid& g, typename C::T* ring, int slot, int e,
+                                           long long gx, long long gy, long long gz, bool out_y,
+                                           bool out_z) {
+  typedef typename C::T T;
+  const int hz = g.halo[0], hy = g.halo[1], hx = g.halo[2];
+  const int nz = g.interior[0], ny = g.interior[1], nx = g.interior[2];
+  const bool out_x = (gx < hx || gx >= hx + nx) && g.dims[2] > 1;
+#pragma unroll
+  for (int f = 0; f < C::NIN; ++f) {
+    T v;
+    if (C::BC == CSD_BC_DIRICHLET) {
+      v = (T)g.bc_value;
+    } else {
+      const long long mx = out_x ? bc_map(gx, hx, nx, C::BC) : gx;
+      const long long my = out_y ? bc_map(gy, hy, ny, C::BC) : gy;
+      const long long mz = out_z ? bc_map(gz, hz, nz, C::BC) : gz;
+      v = reinterpret_cast<const T*>(g.in[f])[mz * g.pitch_z + my * g.pitch_y + mx];
+      if (C::BC == CSD_BC_REFLECTING) {
+        // internal dims (Z, Y, X) <- array dims; bc_odd uses array dim numbers
+        const int odd = g.bc_odd[f];
+        const int nd = g.ndim;
+        bool flip = false;
+        if (nd == 3) flip = ((odd & 1) && out_z) ^ ((odd & 2) && out_y) ^ ((odd & 4) && out_x);
+        else if (nd == 2) flip = ((odd & 1) && out_z) ^ ((odd & 2) && out_x);
+        else flip = (odd & 1) && out_x;
+        if (flip) v = -v;
+      }
+    }
+    ring[(f * C::NSLOT + slot) * C::SLOT_ELEMS + e] = v;
+  }
+}
+
 template <class C>
 __device__ __forceinline__ void patch_boundary(const csd_grid& g, typename C::T* ring, int slot,
                                                int x0, int y0, int z0) {
-  typedef typename C::T T;
   const int hz = g.halo[0], hy = g.halo[1], hx = g.halo[2];
   const int nz = g.interior[0], ny = g.interior[1], nx = g.interior[2];
   const bool edge = x0 < hx || x0 + C::BOXW > hx + nx || y0 < hy || y0 + C::BOXH > hy + ny ||
                     z0 < hz || z0 + C::ROWS > hz + nz;
   if (!edge) return;
-  constexpr int N = C::ROWS * C::BOXH * C::BOXW;
-  for (int e = threadIdx.x; e < N; e += C::NT) {
-    const int xx = e % C::BOXW;
-    const int t = e / C::BOXW;
-    const int yy = t % C::BOXH;
-    const int rr = t / C::BOXH;
-    const long long gx = (long long)x0 + xx, gy = (long long)y0 + yy, gz = (long long)z0 + rr;
-    const bool inside = gx >= hx && gx < hx + nx && gy >= hy && gy < hy + ny && gz >= hz &&
-                        gz < hz + nz;
-    if (inside) continue;
-    // cells beyond the array's own extent are never read by interior points
-    if (gx < 0 || gy < 0 || gz < 0 || gx >= g.dims[2] || gy >= g.dims[1] || gz >= g.dims[0])
-      continue;
-    const bool out_x = (gx < hx || gx >= hx + nx) && g.dims[2] > 1;
+  constexpr int LINES = C::ROWS * C::BOXH;
+  constexpr int NW = C::NT / 32;
+  const int lane = threadIdx.x & 31;
+  // cells beyond the array's own extent are never read by interior points
+  const int xa = x0 < 0 ? -x0 : 0;
+  const long long xe = g.dims[2] - (long long)x0;
+  const int xb = xe < C::BOXW ? (int)xe : C::BOXW;
+  for (int line = threadIdx.x >> 5; line < LINES; line += NW) {
+    const int yy = line % C::BOXH;
+    const int rr = line / C::BOXH;
+    const long long gy = (long long)y0 + yy, gz = (long long)z0 + rr;
+    if (gy < 0 || gz < 0 || gy >= g.dims[1] || gz >= g.dims[0]) continue;
     const bool out_y = (gy < hy || gy >= hy + ny) && g.dims[1] > 1;
     const bool out_z = (gz < hz || gz >= hz + nz) && g.dims[0] > 1;
-#pragma unroll
-    for (int f = 0; f < C::NIN; ++f) {
-      T v;
-      if (C::BC == CSD_BC_DIRICHLET) {
-        v = (T)g.bc_value;
-      } else {
-        const long long mx = out_x ? bc_map(gx, hx, nx, C::BC) : gx;
-        const long long my = out_y ? bc_map(gy, hy, ny, C::BC) : gy;
-        const long long mz = out_z ? bc_map(gz, hz, nz, C::BC) : gz;
-        v = reinterpret_cast<const T*>(g.in[f])[mz * g.pitch_z + my * g.pitch_y + mx];
-        if (C::BC == CSD_BC_REFLECTING) {
-          // internal dims (Z, Y, X) <- array dims; bc_odd uses array dim numbers
-          const int odd = g.bc_odd[f];
-          const int nd = g.ndim;
-          bool flip = false;
-          if (nd == 3) flip = ((odd & 1) && out_z) ^ ((odd & 2) && out_y) ^ ((odd & 4) && out_x);
-          else if (nd == 2) flip = ((odd & 1) && out_z) ^ ((odd & 2) && out_x);
-          else flip = (odd & 1) && out_x;
-          if (flip) v = -v;
-        }
-      }
-      ring[(f * C::NSLOT + slot) * C::SLOT_ELEMS + e] = v;
+    const int ebase = line * C::BOXW;
+    if (out_y || out_z) {
+      for (int xx = xa + lane; xx < xb; xx += 32)
+        patch_cell<C>(g, ring, slot, ebase + xx, (long long)x0 + xx, gy, gz, out_y, out_z);
+    } else {
+      // left: [xa, hx - x0), right: [hx + nx - x0, xb)
+      const int l1 = min(xb, hx - x0);
+      for (int xx = xa + lane; xx < l1; xx += 32)
+        patch_cell<C>(g, ring, slot, ebase + xx, (long long)x0 + xx, gy, gz, false, false);
+      for (int xx = max(xa, hx + nx - x0) + lane; xx < xb; xx += 32)
+        patch_cell<C>(g, ring, slot, ebase + xx, (long long)x0 + xx, gy, gz, false, false);
     }
   }
   // the slot will be refilled by TMA (async proxy) after these generic writes

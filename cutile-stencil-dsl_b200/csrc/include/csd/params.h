@@ -81,7 +81,8 @@ typedef struct csd_kernel_desc {
   int halo_chunks;
   int pad_left, box_w, box_h;
   int smem_bytes;
-  int zchunk;        // default Z rows per work item (0 = sized at launch)
+  int zchunk;        // default Z rows per work item (0 = sized at launch for one
+                     // item per resident block, -W = W items per resident block)
   int temporal;      // stencil steps per pass
   int bc_mode;       // CSD_BC_* fused into the staging (0 = none)
   int min_blocks;

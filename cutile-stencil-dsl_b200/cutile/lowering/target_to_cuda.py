@@ -114,8 +114,10 @@ class _BodyEmitter:
             ct = _CTYPE[typ]
             tgt = "f64" if typ in ("w", "f64") else typ
             sfx = "f" if tgt == "f32" else "d"
-            if op in ("addf", "subf", "mulf", "divf"):
-                fn = {"addf": "add", "subf": "sub", "mulf": "mul", "divf": "div"}[op]
+            if op == "divf":
+                expr = f"csd::div_rn({self.conv(args[0], tgt)}, {self.conv(args[1], tgt)})"
+            elif op in ("addf", "subf", "mulf"):
+                fn = {"addf": "add", "subf": "sub", "mulf": "mul"}[op]
                 expr = f"__{sfx}{fn}_rn({self.conv(args[0], tgt)}, {self.conv(args[1], tgt)})"
             elif op == "cast":
                 expr = self.conv(args[0], tgt)
@@ -124,7 +126,7 @@ class _BodyEmitter:
             elif op == "absf":
                 expr = f"{'fabsf' if tgt == 'f32' else 'fabs'}({self.conv(args[0], tgt)})"
             elif op == "sqrt":
-                expr = f"__{sfx}sqrt_rn({self.conv(args[0], tgt)})"
+                expr = f"csd::sqrt_rn({self.conv(args[0], tgt)})"
             elif op in ("maxf", "minf"):
                 fn = "csd_max" if op == "maxf" else "csd_min"
                 expr = f"{fn}({self.conv(args[0], tgt)}, {self.conv(args[1], tgt)})"
@@ -247,7 +249,8 @@ def engine_params(kernel: KernelOp) -> dict:
         "NT": int(hints.get("threads", 256)), "STAGES": int(hints.get("stages", 1)),
         "TEMPORAL": kernel.temporal_steps.data if kernel.temporal_steps is not None else 1,
         "BC": BC_CODES[kernel.boundary_mode.data if kernel.boundary_mode is not None else "none"],
-        "MINB": int(hints.get("min_blocks", 1)), "ZCHUNK": int(hints.get("zchunk", 0)),
+        "MINB": int(hints.get("min_blocks", 1)), "ZCHUNK": (int(hints.get("zchunk", 0)) if int(hints.get("zchunk", 0)) > 0
+                   else -int(hints.get("waves", 1)) if int(hints.get("waves", 1)) > 1 else 0),
         "ndim": ndim,
         "NSCAL": kernel.scalar_count.data if kernel.scalar_count is not None else 0,
         "NDYN": kernel.dyn_count.data if kernel.dyn_count is not None else 0,

@@ -271,9 +271,12 @@ def _plan_from(tile_sizes, kernel_hints, ndim, base_plan):
             p = replace(p, tile_x=t[0])
     if kernel_hints:
         kw = {}
-        for k in ("threads", "stages", "zchunk"):
+        for k in ("threads", "stages", "zchunk", "waves"):
             if k in kernel_hints:
                 kw[k] = int(kernel_hints[k])
+        occ = kernel_hints.get("min_blocks", kernel_hints.get("occupancy"))
+        if occ is not None:
+            kw["occupancy"] = int(occ)
         p = replace(p, **kw)
     assert isinstance(p, EnginePlan)
     return p
@@ -420,6 +423,8 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
         # blocked there either; it advances one step per launch.
         T = 1
     plan = _plan_from(tile_sizes, kernel_hints, len(stencil_halo), replace(plan, temporal=T))
+    if occupancy is not None:
+        plan = replace(plan, occupancy=int(occupancy))
     plan = fit_plan(plan, stencil_halo, dtype_bytes, num_inputs, analysis.get("body_ops", 0))
     hints = plan.hints()
     if occupancy is not None:
@@ -438,7 +443,8 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
     cuda = emit_cuda(target)
     kernels = {"main": name}
     if boundary_spec is not None:
-        bc_plan = fit_plan(replace(plan, temporal=1), stencil_halo, dtype_bytes, num_inputs)
+        bc_plan = fit_plan(replace(plan, temporal=1), stencil_halo, dtype_bytes, num_inputs,
+                           analysis.get("body_ops", 0))
         bc_target = lower_to_target_ir(ir.clone(), bc_plan.tile_sizes(), halo_widths,
                                        temporal_steps=1, boundary_spec=boundary_spec,
                                        kernel_hints=bc_plan.hints(), dtype=dtype,
@@ -562,8 +568,11 @@ def compile_fused(stencil_fns: list, domain: tuple[int, ...] | None = None, hw=N
     num_loads = len(meta.accesses)
     plan = default_engine_plan(ndim, num_loads, dtype_bytes, stencil_halo, meta.num_inputs,
                                meta.num_outputs)
-    plan = fit_plan(_plan_from(tile_sizes, kernel_hints, ndim, plan), stencil_halo, dtype_bytes,
-                    meta.num_inputs)
+    plan = _plan_from(tile_sizes, kernel_hints, ndim, plan)
+    if occupancy is not None:
+        plan = replace(plan, occupancy=int(occupancy))
+    body_ops = sum(sum(1 for _ in m.walk()) for m in modules)
+    plan = fit_plan(plan, stencil_halo, dtype_bytes, meta.num_inputs, body_ops)
     hints = plan.hints()
     if occupancy is not None:
         hints["occupancy"] = occupancy

@@ -196,8 +196,9 @@ class NativeKernel:
                 "blocks_per_sm": blocks.value}
 
 
-def field_of(t) -> Field:
-    """csd_field for a torch tensor (must be on CUDA, float32/float64, contiguous)."""
+def field_of(t, pitched: bool = False) -> Field:
+    """csd_field for a torch tensor (CUDA, float32/float64, C-contiguous; with
+    ``pitched`` also a row-pitched view: unit innermost stride, padded rows)."""
     import torch
 
     if not isinstance(t, torch.Tensor):
@@ -213,7 +214,8 @@ def field_of(t) -> Field:
     if t.dim() < 1 or t.dim() > 3:
         raise ValueError("fields must be 1-, 2- or 3-D")
     if not t.is_contiguous():
-        raise ValueError("fields must be C-contiguous")
+        if not pitched or t.stride(-1) != 1:
+            raise ValueError("fields must be C-contiguous")
     f = Field()
     f.ptr = t.data_ptr()
     f.ndim = t.dim()
@@ -257,8 +259,8 @@ def make_opts(halo, *, zchunk: int = 0, grid: int = 0, loader: int = -1, bc_valu
 
 def launch(kernel: NativeKernel, inputs, outputs, halo, stream=None, **kw) -> None:
     lib = library()
-    fin = (Field * len(inputs))(*[field_of(t) for t in inputs])
-    fout = (Field * len(outputs))(*[field_of(t) for t in outputs])
+    fin = (Field * len(inputs))(*[field_of(t, True) for t in inputs])
+    fout = (Field * max(1, len(outputs)))(*[field_of(t, True) for t in outputs])
     o = make_opts(halo, **kw)
     check(lib.csd_launch(kernel.handle, fin, len(inputs), fout, len(outputs), ctypes.byref(o),
                          ctypes.c_void_p(stream_handle(stream))))
@@ -272,8 +274,8 @@ def grid_build(kernel: NativeKernel, inputs, outputs, halo, dest, **kw) -> tuple
     """Write the descriptor of one batched grid into host buffer ``dest``
     (a ctypes buffer of ``grid_size()`` bytes); returns (work items, loader)."""
     lib = library()
-    fin = (Field * len(inputs))(*[field_of(t) for t in inputs])
-    fout = (Field * max(1, len(outputs)))(*[field_of(t) for t in outputs])
+    fin = (Field * len(inputs))(*[field_of(t, True) for t in inputs])
+    fout = (Field * max(1, len(outputs)))(*[field_of(t, True) for t in outputs])
     o = make_opts(halo, **kw)
     items = ctypes.c_int()
     loader = ctypes.c_int()

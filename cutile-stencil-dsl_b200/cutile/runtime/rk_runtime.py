@@ -59,7 +59,10 @@ class RKProgram:
         if ws is None:
             names = {n for row in self.table for n in (row[4], row[5], row[6], row[7])
                      if n not in (None, "u")}
-            ws = {n: tuple(torch.zeros_like(x) for x in state) for n in sorted(names)}
+            # same strides as the state (row-pitched batches included)
+            ws = {n: tuple(torch.empty_strided(x.size(), x.stride(), dtype=x.dtype,
+                                               device=x.device).zero_() for x in state)
+                  for n in sorted(names)}
             self._work[key] = ws
         return ws
 
@@ -117,6 +120,43 @@ class RKProgram:
                 dst[inner].copy_(src[inner])
 
 
+def pack_grids(shapes, nfields: int, dtype, device, row_align_bytes: int = 128):
+    """Fields of many grids in one flat device buffer, rows padded to
+    ``row_align_bytes`` so that every grid qualifies for the TMA loader and
+    16-byte vector stores.  Returns ``(flat, grids)``: ``grids[g]`` is a tuple
+    of ``nfields`` row-pitched views of shape ``shapes[g]`` (halo included);
+    the pad columns are never read or written by the engine."""
+    import torch
+
+    esz = torch.empty((), dtype=dtype).element_size()
+    align = max(1, row_align_bytes // esz)
+    layout, total = [], 0
+    for shp in shapes:
+        shp = tuple(int(x) for x in shp)
+        pitch = -(-shp[-1] // align) * align
+        outer = 1
+        for x in shp[:-1]:
+            outer *= x
+        span = outer * pitch
+        offs = []
+        for _ in range(nfields):
+            offs.append(total)
+            total += -(-span * esz // 256) * 256 // esz
+        layout.append((shp, pitch, offs))
+    flat = torch.zeros(max(total, 1), dtype=dtype, device=device)
+    grids = []
+    for shp, pitch, offs in layout:
+        strides, acc = [1], pitch
+        for x in reversed(shp[1:-1]):
+            strides.insert(0, acc)
+            acc *= x
+        if len(shp) > 1:
+            strides.insert(0, acc)
+        strides = tuple(strides[-len(shp):])
+        grids.append(tuple(flat.as_strided(shp, strides, off) for off in offs))
+    return flat, grids
+
+
 class BatchLaunch:
     """Device descriptors of one kernel over many grids (one persistent launch)."""
 
@@ -160,6 +200,14 @@ class BatchLaunch:
                             self.ngrids, self.total_items, stream, grid=grid, loader=self.loader)
 
 
+def _batch_zchunk(kernel: native.NativeKernel) -> int:
+    """Rows per work item in a batch: short items for issue-bound bodies
+    (kernels whose default asks for several items per resident block), long
+    ones for memory-bound bodies."""
+    d = kernel.desc
+    return 2 * d["rows"] if d["zchunk"] < 0 else 64
+
+
 class RKBatch:
     """Many independent grids advanced together, one launch per stage.
 
@@ -172,7 +220,7 @@ class RKBatch:
     """
 
     def __init__(self, rk_result, states: list, scalars: list | None = None, *, dt=None,
-                 cfl=None, bc_odd=(), bc_value: float = 0.0, zchunk: int = 64,
+                 cfl=None, bc_odd=(), bc_value: float = 0.0, zchunk: int | None = None,
                  dt_max: float = 1e30):
         import torch
 
@@ -200,8 +248,9 @@ class RKBatch:
                 per.append({"inputs": inputs, "outputs": outputs,
                             "scalars": self.prog._scalars(scalars[g]),
                             "dyn": self.dt.data_ptr() + 8 * g, "bc_odd": bc_odd})
-            self.stage_launches.append(BatchLaunch(self.prog.kernel(k), per,
-                                                   self.prog.spec["halo"], zchunk=zchunk,
+            kern = self.prog.kernel(k)
+            self.stage_launches.append(BatchLaunch(kern, per, self.prog.spec["halo"],
+                                                   zchunk=zchunk or _batch_zchunk(kern),
                                                    bc_value=bc_value))
         self.speed_launch = None
         if cfl is not None:
@@ -209,8 +258,9 @@ class RKBatch:
             self.scale = torch.as_tensor(scale, dtype=torch.float64, device=dev)
             per = [{"inputs": list(st[:m]), "outputs": [], "red": self.smax.data_ptr() + 8 * g}
                    for g, st in enumerate(self.states)]
-            self.speed_launch = BatchLaunch(speed_program.kernel("main"), per,
-                                            speed_program.spec["halo"], zchunk=zchunk)
+            kern = speed_program.kernel("main")
+            self.speed_launch = BatchLaunch(kern, per, speed_program.spec["halo"],
+                                            zchunk=zchunk or _batch_zchunk(kern))
         last_out = self.prog.table[-1][7]
         if last_out != "u":
             raise NotImplementedError("batched stepping needs a method whose last stage writes "
@@ -243,4 +293,4 @@ class RKBatch:
         return g
 
 
-__all__ = ["RKProgram", "RKBatch", "BatchLaunch"]
+__all__ = ["RKProgram", "RKBatch", "BatchLaunch", "pack_grids"]
