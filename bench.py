@@ -615,6 +615,235 @@ def run_sw_batch(args) -> dict | None:
     return line if rank == 0 else None
 
 
+# ---------------------------------------------------------------------------
+# Gray-Scott: 4096^2 periodic, fused u/v kernel, FP64 vs FP32 vs FP32+Kahan
+# ---------------------------------------------------------------------------
+GS_N = 4096
+GS_STEPS = 10000
+GS_METRIC = "GPts/s (2-D Gray-Scott 4096^2 periodic, fused u/v step, FP32 + Kahan)"
+
+
+def _gs_fused(precision: str):
+    import cutile
+    import stencil_defs as D
+    from cutile import stencil
+
+    return cutile.compile_fused([stencil(ndim=2)(D.gs_u), stencil(ndim=2)(D.gs_v)],
+                                precision=precision, boundary="periodic")
+
+
+def _gs_cpu_job(args):
+    n, steps, seed = args
+    import numpy as np
+
+    import stencil_defs as D
+    from oracle import stencil_oracle as O
+
+    u, v = D.gray_scott_init(n, seed=seed, halo=(1, 1))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        u, v = (O.stencil_with_boundary([u, v], D.gs_u, 2, (1, 1), "periodic"),
+                O.stencil_with_boundary([u, v], D.gs_v, 2, (1, 1), "periodic"))
+    return time.perf_counter() - t0, n * n * steps
+
+
+def gs_cpu_baseline(cores: int, n: int = 1024, steps: int = 3) -> dict:
+    """The oracle (NumPy restatement of apply_boundary + apply_stencil for
+    both fields) on ``cores`` processes, each a seeded n^2 periodic grid."""
+    import multiprocessing as mp
+
+    if cores == 1:
+        secs, pts = _gs_cpu_job((n, steps, 2))
+        rate, wall = pts / secs, secs
+    else:
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(cores) as pool:
+            pool.map(_gs_cpu_job, [(64, 1, k) for k in range(cores)])
+            t0 = time.perf_counter()
+            res = pool.map(_gs_cpu_job, [(n, steps, 2 + k) for k in range(cores)])
+            wall = time.perf_counter() - t0
+        rate = sum(p for _, p in res) / wall
+    return {"value": round(rate / 1e9, 5), "unit": "GPts/s", "cores": cores, "kind": "port",
+            "sample": f"{cores} x {steps} fused u/v steps of a {n}^2 periodic float64 grid "
+                      f"(oracle stencil_with_boundary, wall {wall:.1f} s)"}
+
+
+def run_gray_scott(args) -> dict | None:
+    import numpy as np
+    import torch
+
+    import stencil_defs as D
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if world > 1:
+        torch.distributed.init_process_group("nccl", init_method="env://")
+    stream = torch.cuda.current_stream()
+    steps = args.steps
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    runs = {}
+    for prec in ("fp64", "fp32", "fp32_kahan"):
+        r = _gs_fused(prec)
+        h = r.halo_widths
+        dtype = "float64" if prec == "fp64" else "float32"
+        u0, v0 = D.gray_scott_init(GS_N, seed=2 + rank, halo=h, dtype=dtype)
+        step = getattr(r.load_module(), f"step_{r.name}")
+        a = [torch.from_numpy(u0).cuda(), torch.from_numpy(v0).cuda()]
+        b = [torch.zeros_like(a[0]), torch.zeros_like(a[1])]
+        kahan = prec == "fp32_kahan"
+        ca = [torch.zeros_like(a[0]), torch.zeros_like(a[1])] if kahan else []
+        cb = [torch.zeros_like(a[0]), torch.zeros_like(a[1])] if kahan else []
+        init = [x.clone() for x in a]
+
+        def run(n):
+            nonlocal a, b, ca, cb
+            for _ in range(n):
+                if kahan:
+                    step(*a, *ca, *b, *cb)
+                    ca, cb = cb, ca
+                else:
+                    step(*a, *b)
+                a, b = b, a
+
+        run(args.warmup)
+        for x, y in zip(a, init):
+            x.copy_(y)
+        for c in ca:
+            c.zero_()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        if prec == "fp32_kahan":
+            clk = ClockSampler(local).__enter__()
+        barrier()
+        ev0.record(stream)
+        run(steps)
+        ev1.record(stream)
+        barrier()
+        if prec == "fp32_kahan":
+            clk.__exit__(None, None, None)
+            clocks = clk.summary()
+        ms = ev0.elapsed_time(ev1)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        inner = tuple(slice(x, sz - x) for x, sz in zip(h, u0.shape))
+        runs[prec] = {"ms": ms, "u": a[0][inner].double(), "v": a[1][inner].double(),
+                      "itemsize": np.dtype(dtype).itemsize, "h": h, "step": step,
+                      "state": (a, ca), "init": init}
+
+    def rel(x, y):
+        return float(torch.linalg.norm(x - y) / torch.linalg.norm(y))
+
+    ref = runs["fp64"]
+    err = {p: {"u": rel(runs[p]["u"], ref["u"]), "v": rel(runs[p]["v"], ref["v"])}
+           for p in ("fp32", "fp32_kahan")}
+    npts = GS_N * GS_N
+    gpts = {p: npts * steps / (runs[p]["ms"] / 1e3) / 1e9 * world for p in runs}
+    k = runs["fp32_kahan"]
+    ms_step = k["ms"] / steps
+    # algorithmic bytes per launch: u, v, c_u, c_v read once and written once
+    alg_bytes = 8 * 4 * npts
+    achieved = alg_bytes / (ms_step / 1e3) / 1e9
+    peak, peak_kind = _peaks()
+
+    # end-to-end through the public step function: pinned host u, v (and
+    # zero compensation) -> device, the whole solve, u, v -> host
+    (a, ca), init = k["state"], k["init"]
+    host_in = [x.cpu().pin_memory() for x in init]
+    host_out = [torch.empty_like(x).pin_memory() for x in host_in]
+    e2e_steps = min(steps, 1000)
+    step = k["step"]
+    b = [torch.zeros_like(a[0]), torch.zeros_like(a[1])]
+    cb = [torch.zeros_like(a[0]), torch.zeros_like(a[1])]
+    barrier()
+    t0 = time.perf_counter()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for x, y in zip(a, host_in):
+        x.copy_(y, non_blocking=True)
+    for c in ca:
+        c.zero_()
+    for _ in range(e2e_steps):
+        step(*a, *ca, *b, *cb)
+        a, b, ca, cb = b, a, cb, ca
+    for x, y in zip(host_out, a):
+        x.copy_(y, non_blocking=True)
+    e1.record(stream)
+    barrier()
+    e2e_ms = max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3)
+    e2e = npts * e2e_steps / (e2e_ms / 1e3) / 1e9 * world
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = gs_cpu_baseline(os.cpu_count() or 1)
+    line = {
+        "metric": GS_METRIC, "value": round(gpts["fp32_kahan"], 3), "unit": "GPts/s",
+        "n_gpus": world, "steps": steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 5),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 + f32 compensation", "data": "synthetic",
+        "config": {"workload": f"Gray-Scott u/v, Du=0.16 Dv=0.08 F=0.037 k=0.06 dt=1, {GS_N}^2 "
+                               f"periodic (fused into staging), u=1 v=0 plus 20 noisy 32^2 "
+                               f"squares (seed 2); one step = one compile_fused launch of both "
+                               f"fields with Kahan-compensated updates; {steps} steps from the "
+                               f"initial state",
+                   "l2": "fields 4 x 67 MB + outputs > 126 MB L2",
+                   "parallelism": f"replicas{world}"},
+        "comparison": {
+            "fp64_gpts": round(gpts["fp64"], 3), "fp32_gpts": round(gpts["fp32"], 3),
+            "fp32_kahan_gpts": round(gpts["fp32_kahan"], 3),
+            "rel_l2_vs_fp64_after_steps": err,
+            "oracle": "the GPU FP64 path, bit-exact to the NumPy oracle on 50-step runs of "
+                      "the same stencils (parity tests)"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": peak_kind,
+                     "kernel": "fused u/v Kahan step",
+                     "algorithmic_bytes_per_launch": alg_bytes},
+        "e2e": {"value": round(e2e, 3), "unit": "GPts/s",
+                "h2d_bytes_per_step": int(sum(x.numel() * 4 for x in host_in)),
+                "d2h_bytes_per_step": int(sum(x.numel() * 4 for x in host_out)),
+                "step": f"H2D of u, v; {e2e_steps} Kahan steps; D2H of u, v"},
+        "gpu_launches": steps,
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return line if rank == 0 else None
+
+
+def run_gs_reference(args) -> dict | None:
+    world, rank, _ = _dist()
+    if rank != 0:
+        return None
+    cores = os.cpu_count() or 1
+    vals = []
+    for k in range(args.warmup + args.steps):
+        cb = gs_cpu_baseline(cores, n=512, steps=1)
+        if k >= args.warmup:
+            vals.append(cb["value"])
+    value = statistics.median(vals)
+    cb["value"] = value
+    return {
+        "metric": GS_METRIC, "value": value, "unit": "GPts/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(GS_N * GS_N / (value * 1e9) * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": f"Gray-Scott {GS_N}^2 periodic fused u/v step, CPU NumPy oracle "
+                               f"on {cores} processes, 512^2 samples"},
+        "cpu_baseline": cb,
+        "e2e": {"value": value, "unit": "GPts/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
 def run_sw_reference(args) -> dict | None:
     world, rank, _ = _dist()
     if rank != 0:
@@ -646,16 +875,16 @@ def run_sw_reference(args) -> dict | None:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--dtype", choices=("float64", "float32"), default="float64")
     ap.add_argument("--temporal", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--n", type=int, default=512, help="interior extent per dimension")
-    ap.add_argument("--workload", choices=("lap7", "sw_batch"), default="lap7",
+    ap.add_argument("--workload", choices=("lap7", "sw_batch", "gray_scott"), default="lap7",
                     help="lap7: 3-D 7-point 512^3 sweeps; sw_batch: 256 batched shallow-water "
-                         "solves")
+                         "solves; gray_scott: 4096^2 fused Gray-Scott, FP64/FP32/Kahan")
     ap.add_argument("--sw-grids", type=int, default=256, help="sw_batch: number of grids")
     ap.add_argument("--sw-n", type=int, default=0,
                     help="sw_batch: fixed grid size (0 = log-uniform in [64, 2048])")
@@ -665,13 +894,22 @@ def main() -> None:
     ap.add_argument("--no-compare", dest="compare", action="store_false",
                     help="sw_batch: time the FP32 batch only (profiling cases)")
     args = ap.parse_args()
+    args.steps_given = args.steps
+    if args.steps is None:
+        args.steps = 50
     global N_INTERIOR, SW_GRIDS, SW_FIXED_N, SW_STEPS, SW_ZCHUNK
     N_INTERIOR = args.n
     SW_GRIDS, SW_FIXED_N, SW_STEPS = args.sw_grids, args.sw_n, args.sw_steps
     SW_ZCHUNK = args.sw_zchunk
     if args.warmup < 3:
         args.warmup = 3
-    if args.workload == "sw_batch":
+    if args.workload == "gray_scott":
+        if args.steps_given is None:
+            args.steps = GS_STEPS if args.impl == "ours" else 3
+        line = run_gs_reference(args) if args.impl == "reference" else run_gray_scott(args)
+    elif args.workload == "sw_batch":
+        if args.steps_given is None:
+            args.steps = 3
         line = run_sw_reference(args) if args.impl == "reference" else run_sw_batch(args)
     else:
         line = run_reference(args) if args.impl == "reference" else run_ours(args)

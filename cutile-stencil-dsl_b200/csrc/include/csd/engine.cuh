@@ -346,13 +346,9 @@ __device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
             (unsigned long long)__double_as_longlong(v));
 }
 
-// Grid and local item of global work item `item` (batched: binary search of
-// the items prefix; single grid: the inline descriptor).
-__device__ __forceinline__ const csd_grid& grid_of(const csd_params& p, int item, int& local) {
-  if (p.grids == nullptr) {
-    local = item;
-    return p.g;
-  }
+// Grid of global work item `item` in a batch: binary search of the items
+// prefix; `local` receives the item's index within its grid.
+__device__ __forceinline__ int batch_grid_of(const csd_params& p, int item, int& local) {
   int lo = 0, hi = p.ngrids - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
@@ -360,12 +356,19 @@ __device__ __forceinline__ const csd_grid& grid_of(const csd_params& p, int item
     else hi = mid - 1;
   }
   local = item - p.item_start[lo];
-  return p.grids[lo];
+  return lo;
 }
 
 // ---------------------------------------------------------------------------
 // The engine
 // ---------------------------------------------------------------------------
+template <class C, class Body, bool BATCHED>
+__device__ __forceinline__ void engine_items(const csd_params& p, typename C::T* ring,
+                                             typename C::T* inter, unsigned long long* bars,
+                                             int& abort_flag, double* red_warp);
+
+// Single-grid launches read the descriptor from the kernel parameters
+// (constant bank operands); batched launches from the device work list.
 template <class C, class Body>
 __device__ __forceinline__ void stream_engine(const csd_params& p) {
   typedef typename C::T T;
@@ -390,15 +393,25 @@ __device__ __forceinline__ void stream_engine(const csd_params& p) {
   // garbage that could be mistaken for data by a debugging reader.
   for (int e = threadIdx.x; e < C::INTER_ELEMS; e += C::NT) inter[e] = T(0);
   __syncthreads();
+  if (p.grids == nullptr)
+    engine_items<C, Body, false>(p, ring, inter, bars, abort_flag, red_warp);
+  else
+    engine_items<C, Body, true>(p, ring, inter, bars, abort_flag, red_warp);
+}
 
+template <class C, class Body, bool BATCHED>
+__device__ __forceinline__ void engine_items(const csd_params& p, typename C::T* ring,
+                                             typename C::T* inter, unsigned long long* bars,
+                                             int& abort_flag, double* red_warp) {
+  typedef typename C::T T;
   constexpr int T_ = C::TEMPORAL;
   constexpr int HCT = C::HC * T_;  // input halo chunks per side for the whole chain
   unsigned seq = 0;                // chunks consumed by this CTA so far
-  const int total = p.grids == nullptr ? p.g.items : p.total_items;
+  const int total = BATCHED ? p.total_items : p.g.items;
 
   for (int gitem = blockIdx.x; gitem < total; gitem += gridDim.x) {
-    int item;
-    const csd_grid& g = grid_of(p, gitem, item);
+    int item = gitem;
+    const csd_grid& g = BATCHED ? p.grids[batch_grid_of(p, gitem, item)] : p.g;
     const int hz = g.halo[0], hy = g.halo[1], hx = g.halo[2];
     const int nz = g.interior[0], ny = g.interior[1], nx = g.interior[2];
     const int tx = item % g.tiles[0];
@@ -416,6 +429,13 @@ __device__ __forceinline__ void stream_engine(const csd_params& p) {
     const int cy = Y0 - T_ * C::RY;
     const int cz = hz + z0 - HCT * C::ROWS;
     double red_acc = 0.0;
+    // output addressing, read once per item (a batch's descriptor is in
+    // global memory and would be re-read after every store otherwise)
+    const long long pitch_y = g.pitch_y, pitch_z = g.pitch_z;
+    const bool vec_store = g.vec_store != 0;
+    T* outp[C::NOUT];
+#pragma unroll
+    for (int f = 0; f < C::NOUT; ++f) outp[f] = reinterpret_cast<T*>(g.out[f]);
 
     // prologue: fill the ring
     const int pre = min(nchunks, C::NSLOT);
@@ -516,12 +536,12 @@ __device__ __forceinline__ void stream_engine(const csd_params& p) {
               }
               continue;
             }
-            const long long rowoff = (long long)gz * g.pitch_z + (long long)gy * g.pitch_y;
+            const long long rowoff = (long long)gz * pitch_z + (long long)gy * pitch_y;
             const bool full = gx0 >= hx && gx0 + C::VEC <= hx + nx;
 #pragma unroll
             for (int f = 0; f < C::NOUT; ++f) {
-              T* out = reinterpret_cast<T*>(g.out[f]) + rowoff;
-              if (full && g.vec_store) {
+              T* out = outp[f] + rowoff;
+              if (full && vec_store) {
                 store_vec(out + gx0, o.v[f]);
               } else {
 #pragma unroll
