@@ -14,51 +14,62 @@ extern "C" int csd_internal_fail(int code, const char* msg);
 
 namespace {
 
+// Source index along one dimension of a halo cell (the interior cell whose
+// value it takes); interior indices map to themselves.
+__device__ __forceinline__ long long fill_src(long long i, long long nd, int h, int bc) {
+  if (i >= h && i < nd - h) return i;
+  const bool high = i >= nd - h;
+  const long long k = high ? i - (nd - h) : i;  // layer 0 .. h-1
+  if (bc == CSD_BC_NEUMANN) return high ? nd - h - 1 : h;
+  if (bc == CSD_BC_PERIODIC) return high ? h + k : nd - 2 * h + k;
+  return high ? nd - h - 1 - k : 2 * h - 1 - k;  // reflecting
+}
+
+// Fill every halo cell of a (d0, d1, d2) array in one launch.  The halo is
+// enumerated as three disjoint boxes (dim-0 halo layers over the whole
+// cross-section; dim-1 layers over the dim-0 interior; dim-2 layers over
+// the dim-0 and dim-1 interior), and each cell maps every out-of-interior
+// dimension to its source independently.  That equals the dimension-by-
+// dimension slab copies of the reference fill (corners take the value of
+// the mirrored interior corner) for all four conditions.
 template <typename T>
-__global__ void fill_dim_kernel(T* u, long long d0, long long d1, long long d2, int dim, int h,
-                                int bc, T value) {
-  // The array is viewed as (d0, d1, d2); `dim` selects the dimension whose
-  // halo is filled.  Each thread owns one halo cell of that dimension.
-  const long long n[3] = {d0, d1, d2};
-  const long long nd = n[dim];
-  long long other = 1;
-  for (int i = 0; i < 3; ++i)
-    if (i != dim) other *= n[i];
-  const long long total = 2LL * h * other;
+__global__ void fill_halo_kernel(T* u, long long d0, long long d1, long long d2, int h0, int h1,
+                                 int h2, int bc, T value) {
+  const long long i0 = d0 - 2LL * h0, i1 = d1 - 2LL * h1;
+  const long long na = 2LL * h0 * d1 * d2;
+  const long long nb = i0 * 2LL * h1 * d2;
+  const long long nc = i0 * i1 * 2LL * h2;
+  const long long total = na + nb + nc;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
-    const long long k2 = e / other;      // 0 .. 2h-1 : which halo layer
-    long long rest = e % other;
-    const bool high = k2 >= h;
-    const long long k = high ? k2 - h : k2;
-    long long idx[3];
-    // rest enumerates the other two dims in order
-    int j = 2;
-    for (int i = 2; i >= 0; --i) {
-      if (i == dim) continue;
-      idx[i] = rest % n[i];
-      rest /= n[i];
-      (void)j;
-    }
-    long long dst_i, src_i;
-    if (!high) {
-      dst_i = k;
-      if (bc == CSD_BC_NEUMANN) src_i = h;
-      else if (bc == CSD_BC_PERIODIC) src_i = nd - 2 * h + k;
-      else src_i = 2 * h - 1 - k;  // reflecting
+    long long a, b, c;
+    if (e < na) {
+      c = e % d2;
+      long long t = e / d2;
+      b = t % d1;
+      const long long l = t / d1;  // 0 .. 2h0-1
+      a = l < h0 ? l : d0 - 2LL * h0 + l;
+    } else if (e < na + nb) {
+      const long long f = e - na;
+      c = f % d2;
+      long long t = f / d2;
+      const long long l = t % (2LL * h1);
+      a = h0 + t / (2LL * h1);
+      b = l < h1 ? l : d1 - 2LL * h1 + l;
     } else {
-      dst_i = nd - h + k;
-      if (bc == CSD_BC_NEUMANN) src_i = nd - h - 1;
-      else if (bc == CSD_BC_PERIODIC) src_i = h + k;
-      else src_i = nd - h - 1 - k;
+      const long long f = e - na - nb;
+      const long long l = f % (2LL * h2);
+      long long t = f / (2LL * h2);
+      b = h1 + t % i1;
+      a = h0 + t / i1;
+      c = l < h2 ? l : d2 - 2LL * h2 + l;
     }
-    idx[dim] = dst_i;
-    const long long dst = (idx[0] * n[1] + idx[1]) * n[2] + idx[2];
+    const long long dst = (a * d1 + b) * d2 + c;
     if (bc == CSD_BC_DIRICHLET) {
       u[dst] = value;
     } else {
-      idx[dim] = src_i;
-      const long long src = (idx[0] * n[1] + idx[1]) * n[2] + idx[2];
+      const long long src =
+          (fill_src(a, d0, h0, bc) * d1 + fill_src(b, d1, h1, bc)) * d2 + fill_src(c, d2, h2, bc);
       u[dst] = u[src];
     }
   }
@@ -73,21 +84,22 @@ int apply_boundary_t(const csd_field* f, const int* halo, int bc, double value, 
     n[off + i] = f->shape[i];
     h3[off + i] = halo[i];
   }
+  long long cells = 0, inner = 1;
   for (int d = 0; d < 3; ++d) {
-    if (h3[d] == 0) continue;
-    if (bc != CSD_BC_DIRICHLET && n[d] - 2 * h3[d] < h3[d])
+    if (h3[d] < 0 || n[d] - 2LL * h3[d] < 1)
+      return csd_internal_fail(CSD_EINVAL, "halo leaves no interior");
+    if (h3[d] > 0 && bc != CSD_BC_DIRICHLET && n[d] - 2 * h3[d] < h3[d])
       return csd_internal_fail(CSD_EINVAL, "boundary fill needs an interior at least as wide as the halo");
-    long long other = 1;
-    for (int i = 0; i < 3; ++i)
-      if (i != d) other *= n[i];
-    const long long total = 2LL * h3[d] * other;
-    int blocks = (int)((total + 255) / 256);
-    if (blocks > 148 * 16) blocks = 148 * 16;
-    fill_dim_kernel<T><<<blocks, 256, 0, s>>>(reinterpret_cast<T*>(f->ptr), n[0], n[1], n[2], d,
-                                              h3[d], bc, (T)value);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return csd_internal_fail(CSD_ELAUNCH, cudaGetErrorString(e));
+    inner *= n[d] - 2LL * h3[d];
   }
+  cells = n[0] * n[1] * n[2] - inner;
+  if (cells == 0) return CSD_OK;
+  long long blocks = (cells + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  fill_halo_kernel<T><<<(int)blocks, 256, 0, s>>>(reinterpret_cast<T*>(f->ptr), n[0], n[1], n[2],
+                                                  h3[0], h3[1], h3[2], bc, (T)value);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return csd_internal_fail(CSD_ELAUNCH, cudaGetErrorString(e));
   return CSD_OK;
 }
 

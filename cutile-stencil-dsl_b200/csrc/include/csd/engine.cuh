@@ -83,7 +83,14 @@ struct Cfg {
   }
   static constexpr int RING_ELEMS = NIN * NSLOT * SLOT_ELEMS;
   static constexpr int INTER_ELEMS = inter_elems_upto(TEMPORAL);
-  static constexpr int BAR_OFFSET = (RING_ELEMS + INTER_ELEMS) * (int)sizeof(T);
+  // Periodic X wrap (TMA loader): the wrapped source cells of a chunk's X
+  // halo lines are copied ahead with cp.async into a per-slot buffer,
+  // indexed ((field * PLINES + line) * 2 + side) * RX + layer.
+  static constexpr int PLINES = ROWS * BOXH;
+  static constexpr int PBUF = (BC == CSD_BC_PERIODIC && LOADER == CSD_LOADER_TMA && RX > 0) ? 1 : 0;
+  static constexpr int PBUF_SLOT = PBUF ? align_up(NIN * PLINES * 2 * RX, 16) : 0;
+  static constexpr int PBUF_ELEMS = NSLOT * PBUF_SLOT;
+  static constexpr int BAR_OFFSET = (RING_ELEMS + INTER_ELEMS + PBUF_ELEMS) * (int)sizeof(T);
   // +128: the dynamic shared-memory base is aligned up to 128 bytes in the kernel
   static constexpr int SMEM_BYTES = BAR_OFFSET + 8 * NSLOT + 64 + 128;
   static_assert(BOXW <= 256 && BOXH <= 256 && ROWS <= 256, "TMA box limit");
@@ -226,6 +233,39 @@ template <class C>
 struct Loader {
   typedef typename C::T T;
 
+  // Warp 0: copy the wrapped (periodic) sources of the chunk's X-halo cells
+  // that an interior point can read into the slot's wrap buffer, then arrive
+  // on the slot barrier once those copies land (32 arrivals per chunk).
+  // Lines outside the interior in Y or Z are left to the synchronous patch.
+  static __device__ __forceinline__ void prefetch_wrap(const csd_grid& g, T* ring, unsigned bar,
+                                                       int slot, int x0, int y0, int z0) {
+    T* pbuf = ring + C::RING_ELEMS + C::INTER_ELEMS + slot * C::PBUF_SLOT;
+    const int hz = g.halo[0], hy = g.halo[1], hx = g.halo[2];
+    const int nz = g.interior[0], ny = g.interior[1], nx = g.interior[2];
+    const bool touches = x0 < hx || x0 + C::BOXW > hx + nx;
+    if (touches) {
+      constexpr int UNITS = C::NIN * C::PLINES * 2 * C::RX;
+      for (int u = threadIdx.x; u < UNITS; u += 32) {
+        const int k = u % C::RX;
+        const int side = (u / C::RX) & 1;
+        const int line = (u / (2 * C::RX)) % C::PLINES;
+        const int f = u / (2 * C::RX * C::PLINES);
+        const int yy = line % C::BOXH;
+        const int rr = line / C::BOXH;
+        const long long gy = (long long)y0 + yy, gz = (long long)z0 + rr;
+        const long long gx = side ? (long long)hx + nx + k : (long long)hx - C::RX + k;
+        const bool ok = gx >= x0 && gx < (long long)x0 + C::BOXW && gx >= 0 && gx < g.dims[2] &&
+                        (gy >= hy && gy < hy + ny) && (gz >= hz && gz < hz + nz);
+        if (ok) {
+          const long long mx = bc_map(gx, hx, nx, CSD_BC_PERIODIC);
+          const T* src = reinterpret_cast<const T*>(g.in[f]) + gz * g.pitch_z + gy * g.pitch_y + mx;
+          ptx::cp_async_zfill<sizeof(T)>(ptx::smem_addr(pbuf + u), src, true);
+        }
+      }
+    }
+    ptx::cp_async_arrive(bar);
+  }
+
   // Issue the copies of one chunk (all fields) of grid `g` into `slot`.
   static __device__ __forceinline__ void issue(const csd_grid& g, T* ring, unsigned bar, int slot,
                                                int x0, int y0, int z0) {
@@ -237,6 +277,9 @@ struct Loader {
           T* dst = ring + (f * C::NSLOT + slot) * C::SLOT_ELEMS;
           ptx::tma_load_3d(ptx::smem_addr(dst), &g.tmap[f], x0, y0, z0, bar);
         }
+      }
+      if constexpr (C::PBUF) {
+        if (threadIdx.x < 32) prefetch_wrap(g, ring, bar, slot, x0, y0, z0);
       }
     } else {
       constexpr int N = C::ROWS * C::BOXH * C::BOXW;
@@ -263,11 +306,24 @@ struct Loader {
 };
 
 // Overwrite the cells of a freshly landed chunk that lie outside the domain
-// interior with their boundary-condition values (fused boundary fill).
-// `bc_odd[f]` bit d: a value mirrored across a boundary of dim d changes
-// sign (a wall's normal momentum); the sign is the product over mirrored dims.
-// One warp per chunk line (Z row, Y row): lines outside the interior in Z or
-// Y are patched whole, the others only in their out-of-interior X ranges.
+// interior, but within the stencil radius of it, with their boundary-
+// condition values (fused boundary fill).  `bc_odd[f]` bit d: a value
+// mirrored across a boundary of dim d changes sign (a wall's normal
+// momentum); the sign is the product over mirrored dims.  One warp per chunk
+// line (Z row, Y row): lines outside the interior in Z or Y take their cells
+// from the mirrored line in global memory; the X-halo cells of interior
+// lines come from the same line in shared memory (Neumann, reflecting), the
+// prefetched wrap buffer (periodic, TMA loader) or global memory (periodic,
+// cp.async loader).
+template <class C>
+__device__ __forceinline__ bool odd_flip(const csd_grid& g, int f, bool out_x, bool out_y,
+                                         bool out_z) {
+  const int odd = g.bc_odd[f];
+  if (g.ndim == 3) return ((odd & 1) && out_z) ^ ((odd & 2) && out_y) ^ ((odd & 4) && out_x);
+  if (g.ndim == 2) return ((odd & 1) && out_z) ^ ((odd & 2) && out_x);
+  return (odd & 1) && out_x;
+}
+
 template <class C>
 __device__ __forceinline__ void patch_cell(const csd_grid& g, typename C::T* ring, int slot, int e,
                                            long long gx, long long gy, long long gz, bool out_y,
@@ -286,18 +342,39 @@ __device__ __forceinline__ void patch_cell(const csd_grid& g, typename C::T* rin
       const long long my = out_y ? bc_map(gy, hy, ny, C::BC) : gy;
       const long long mz = out_z ? bc_map(gz, hz, nz, C::BC) : gz;
       v = reinterpret_cast<const T*>(g.in[f])[mz * g.pitch_z + my * g.pitch_y + mx];
-      if (C::BC == CSD_BC_REFLECTING) {
-        // internal dims (Z, Y, X) <- array dims; bc_odd uses array dim numbers
-        const int odd = g.bc_odd[f];
-        const int nd = g.ndim;
-        bool flip = false;
-        if (nd == 3) flip = ((odd & 1) && out_z) ^ ((odd & 2) && out_y) ^ ((odd & 4) && out_x);
-        else if (nd == 2) flip = ((odd & 1) && out_z) ^ ((odd & 2) && out_x);
-        else flip = (odd & 1) && out_x;
-        if (flip) v = -v;
-      }
+      if (C::BC == CSD_BC_REFLECTING && odd_flip<C>(g, f, out_x, out_y, out_z)) v = -v;
     }
     ring[(f * C::NSLOT + slot) * C::SLOT_ELEMS + e] = v;
+  }
+}
+
+// X-halo cell `xx` (box column) of an interior line: the value from shared
+// memory (same line, wrap buffer) where the condition allows.
+template <class C>
+__device__ __forceinline__ void patch_x_cell(const csd_grid& g, typename C::T* ring, int slot,
+                                             int line, int xx, int x0, long long gy,
+                                             long long gz, int side) {
+  typedef typename C::T T;
+  const int hx = g.halo[2], nx = g.interior[2];
+  const long long gx = (long long)x0 + xx;
+  if (C::BC == CSD_BC_DIRICHLET || (C::BC == CSD_BC_PERIODIC && !C::PBUF)) {
+    patch_cell<C>(g, ring, slot, line * C::BOXW + xx, gx, gy, gz, false, false);
+    return;
+  }
+  const T* pbuf = ring + C::RING_ELEMS + C::INTER_ELEMS + slot * C::PBUF_SLOT;
+  const int k = side ? (int)(gx - hx - nx) : (int)(gx - (hx - C::RX));
+  const int sx = (int)(bc_map(gx, hx, nx, C::BC) - x0);  // source box column (same line)
+#pragma unroll
+  for (int f = 0; f < C::NIN; ++f) {
+    T* slot_base = ring + (f * C::NSLOT + slot) * C::SLOT_ELEMS;
+    T v;
+    if (C::BC == CSD_BC_PERIODIC) {
+      v = pbuf[((f * C::PLINES + line) * 2 + side) * C::RX + k];
+    } else {
+      v = slot_base[line * C::BOXW + sx];
+      if (C::BC == CSD_BC_REFLECTING && odd_flip<C>(g, f, true, false, false)) v = -v;
+    }
+    slot_base[line * C::BOXW + xx] = v;
   }
 }
 
@@ -309,31 +386,37 @@ __device__ __forceinline__ void patch_boundary(const csd_grid& g, typename C::T*
   const bool edge = x0 < hx || x0 + C::BOXW > hx + nx || y0 < hy || y0 + C::BOXH > hy + ny ||
                     z0 < hz || z0 + C::ROWS > hz + nz;
   if (!edge) return;
-  constexpr int LINES = C::ROWS * C::BOXH;
   constexpr int NW = C::NT / 32;
   const int lane = threadIdx.x & 31;
-  // cells beyond the array's own extent are never read by interior points
-  const int xa = x0 < 0 ? -x0 : 0;
-  const long long xe = g.dims[2] - (long long)x0;
-  const int xb = xe < C::BOXW ? (int)xe : C::BOXW;
-  for (int line = threadIdx.x >> 5; line < LINES; line += NW) {
+  // cells an interior point can read: the interior grown by the radius,
+  // clipped to the array
+  const long long xlo = max((long long)hx - C::RX, 0ll);
+  const long long xhi = min((long long)hx + nx + C::RX, g.dims[2]);
+  const long long ylo = max((long long)hy - C::RY, 0ll);
+  const long long yhi = min((long long)hy + ny + C::RY, g.dims[1]);
+  const long long zlo = max((long long)hz - C::RZ, 0ll);
+  const long long zhi = min((long long)hz + nz + C::RZ, g.dims[0]);
+  const int xa = (int)max(xlo - x0, 0ll);
+  const int xb = (int)min(xhi - x0, (long long)C::BOXW);
+  // interior lines with X-halo cells read from shared memory must see the
+  // landed chunk only (sources are interior cells, never patched)
+  for (int line = threadIdx.x >> 5; line < C::PLINES; line += NW) {
     const int yy = line % C::BOXH;
     const int rr = line / C::BOXH;
     const long long gy = (long long)y0 + yy, gz = (long long)z0 + rr;
-    if (gy < 0 || gz < 0 || gy >= g.dims[1] || gz >= g.dims[0]) continue;
+    if (gy < ylo || gy >= yhi || gz < zlo || gz >= zhi) continue;
     const bool out_y = (gy < hy || gy >= hy + ny) && g.dims[1] > 1;
     const bool out_z = (gz < hz || gz >= hz + nz) && g.dims[0] > 1;
-    const int ebase = line * C::BOXW;
     if (out_y || out_z) {
       for (int xx = xa + lane; xx < xb; xx += 32)
-        patch_cell<C>(g, ring, slot, ebase + xx, (long long)x0 + xx, gy, gz, out_y, out_z);
+        patch_cell<C>(g, ring, slot, line * C::BOXW + xx, (long long)x0 + xx, gy, gz, out_y, out_z);
     } else {
       // left: [xa, hx - x0), right: [hx + nx - x0, xb)
       const int l1 = min(xb, hx - x0);
       for (int xx = xa + lane; xx < l1; xx += 32)
-        patch_cell<C>(g, ring, slot, ebase + xx, (long long)x0 + xx, gy, gz, false, false);
+        patch_x_cell<C>(g, ring, slot, line, xx, x0, gy, gz, 0);
       for (int xx = max(xa, hx + nx - x0) + lane; xx < xb; xx += 32)
-        patch_cell<C>(g, ring, slot, ebase + xx, (long long)x0 + xx, gy, gz, false, false);
+        patch_x_cell<C>(g, ring, slot, line, xx, x0, gy, gz, 1);
     }
   }
   // the slot will be refilled by TMA (async proxy) after these generic writes
@@ -385,7 +468,8 @@ __device__ __forceinline__ void stream_engine(const csd_params& p) {
     abort_flag = 0;
 #pragma unroll 1
     for (int s = 0; s < C::NSLOT; ++s)
-      ptx::mbar_init(ptx::smem_addr(&bars[s]), C::LOADER == CSD_LOADER_TMA ? 1u : (unsigned)C::NT);
+      ptx::mbar_init(ptx::smem_addr(&bars[s]),
+                     C::LOADER == CSD_LOADER_TMA ? 1u + (C::PBUF ? 32u : 0u) : (unsigned)C::NT);
     ptx::fence_mbar_init();
   }
   // Zero the intermediate rings once: rows/columns a stage never writes are
@@ -459,8 +543,12 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
         }
         waited = i;
         if constexpr (C::BC != CSD_BC_NONE) {
-          __syncthreads();
-          if (!abort_flag) patch_boundary<C>(g, ring, slot, cx, cy, cz + i * C::ROWS);
+          // Every thread has seen the chunk land (its own wait), the slot's
+          // previous readers finished before the refill was issued, and the
+          // patch reads only landed interior cells: no barrier is needed
+          // before it.  After a timed-out wait the patch still touches only
+          // in-bounds memory and the block leaves at the barrier below.
+          patch_boundary<C>(g, ring, slot, cx, cy, cz + i * C::ROWS);
         }
       }
       __syncthreads();

@@ -179,7 +179,9 @@ def _align_up(x: int, a: int) -> int:
 
 def engine_geometry(plan: EnginePlan, radius3: tuple[int, int, int], dtype_bytes: int,
                     num_inputs: int) -> dict:
-    """Derived sizes, identical to the constexprs of ``csd::Cfg`` (engine.cuh).
+    """Derived sizes, identical to the constexprs of ``csd::Cfg`` (engine.cuh),
+    except ``smem_bytes``, which always counts the periodic wrap buffer (an
+    upper bound for the other boundary modes).
 
     ``radius3`` is the radius of ONE stencil step per internal dimension
     (Z, Y, X); ``plan.temporal`` steps are chained.
@@ -202,7 +204,9 @@ def engine_geometry(plan: EnginePlan, radius3: tuple[int, int, int], dtype_bytes
     slot_elems = _align_up(plan.rows * box_h * box_w, per128)
     inter = sum(nslot_i * _align_up(plan.rows * (plan.tile_y + 2 * (T - s) * ry) * box_w, per128)
                 for s in range(1, T))
-    smem = (num_inputs * nslot * slot_elems + inter) * dtype_bytes + 8 * nslot + 64 + 128
+    pbuf_slot = _align_up(num_inputs * plan.rows * box_h * 2 * rx, 16) if rx > 0 else 0
+    smem = ((num_inputs * nslot * slot_elems + inter + nslot * pbuf_slot) * dtype_bytes
+            + 8 * nslot + 64 + 128)
     return {"align": align, "pad_left": pad_left, "box_w": box_w, "box_h": box_h,
             "halo_chunks": hc, "nslot": nslot, "slot_elems": slot_elems,
             "smem_bytes": smem}
