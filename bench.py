@@ -844,6 +844,181 @@ def run_gs_reference(args) -> dict | None:
     }
 
 
+# ---------------------------------------------------------------------------
+# Serving: Poisson stream of mixed solves, continuous batching, 150 GB budget
+# ---------------------------------------------------------------------------
+SERVE_REQUESTS = 2000
+SERVE_RATE = 2000.0
+SERVE_BUDGET = 150e9
+SERVE_METRIC = "solves/s (continuous-batching server, Poisson 2000 req/s mixed stencil solves)"
+
+
+def _serve_workload(n: int, rate: float = SERVE_RATE, seed: int = 4, host_init: bool = False):
+    """Seeded request stream: kinds uniform over heat 5-pt / upwind advection /
+    leapfrog wave / 3-D 7-pt, N log-uniform (2-D 64..4096, 3-D 32..256),
+    steps log-uniform 10..1000, float32/float64 50/50, Uniform[0,1) interiors."""
+    import numpy as np
+
+    import stencil_defs as D
+    from cutile.runtime.serving import SolveRequest
+
+    rng = np.random.default_rng(seed)
+    names = list(D.SERVE_KINDS)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+    kind_idx = rng.integers(0, len(names), n)
+    n2 = np.exp(rng.uniform(np.log(64), np.log(4096), n))
+    n3 = np.exp(rng.uniform(np.log(32), np.log(256), n))
+    steps = np.rint(np.exp(rng.uniform(np.log(10), np.log(1000), n))).astype(int)
+    dts = rng.integers(0, 2, n)
+    reqs = []
+    for i in range(n):
+        kind = names[int(kind_idx[i])]
+        ndim, nstate = D.SERVE_KINDS[kind][1], D.SERVE_KINDS[kind][2]
+        m = int(round(n3[i] if ndim == 3 else n2[i]))
+        shape = (m + 2,) * ndim
+        dtype = ("float32", "float64")[int(dts[i])]
+        init = None
+        if host_init:
+            r = np.random.default_rng(4000 + i)
+            u = np.zeros(shape, dtype=dtype)
+            u[(slice(1, -1),) * ndim] = r.random((m,) * ndim, dtype=np.float64).astype(dtype)
+            init = (u,) * nstate
+        reqs.append(SolveRequest(kind, dtype, shape, int(steps[i]), arrival=float(arrivals[i]),
+                                 init=init, seed=4000 + i, rid=i))
+    return reqs
+
+
+def _serve_point_steps(reqs) -> float:
+    tot = 0.0
+    for r in reqs:
+        pts = 1
+        for x in r.shape:
+            pts *= x - 2
+        tot += pts * r.steps
+    return tot
+
+
+def run_serve(args) -> dict | None:
+    import numpy as np
+    import torch
+
+    import stencil_defs as D
+    from cutile.runtime.serving import StencilServer, percentile
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if world > 1:
+        torch.distributed.init_process_group("nccl", init_method="env://")
+    kinds = D.serving_kinds()
+    server = StencilServer(kinds, budget_bytes=SERVE_BUDGET)
+    # warm-up: every (kind, dtype) program loaded and launched
+    warm = _serve_workload(8 * max(1, args.warmup), seed=99)
+    for r in warm:
+        r.steps = 3
+        r.shape = tuple(min(x, 66) for x in r.shape)
+    server.run(warm, realtime=False, keep_state=False)
+    torch.cuda.synchronize()
+
+    reqs = _serve_workload(SERVE_REQUESTS, seed=4 + rank)
+    server.stats = type(server.stats)()
+    if world > 1:
+        torch.distributed.barrier()
+    with ClockSampler(local) as clk:
+        res = server.run(reqs, realtime=True, keep_state=False)
+        torch.cuda.synchronize()
+    clocks = clk.summary()
+    st = server.stats
+    server.stats = type(st)()
+    done = [r for r in res if r.error is None]
+    lat = [r.latency * 1e3 for r in done]
+    span = max(r.completed for r in done) - min(r.arrival for r in reqs)
+    solves_s = len(done) / span
+    if world > 1:
+        t = torch.tensor([span], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        solves_s = len(done) * world / float(t.item())
+    gpts = _serve_point_steps([r for r in reqs]) / span / 1e9
+
+    # each request alone on the plain path (drop-in launch per step), sampled
+    rng = np.random.default_rng(7)
+    sample = sorted(rng.choice(len(reqs), size=min(64, len(reqs)), replace=False).tolist())
+    alone_ms = []
+    for i in sample:
+        _, ms = server.run_alone(reqs[i])
+        alone_ms.append(ms)
+    alone_mean = float(np.mean(alone_ms))
+    # sequential FIFO on the plain path: request k completes after the
+    # alone times of requests 0..k (sample mean), or its arrival, whichever
+    # is later
+    seq_lat, t_free = [], 0.0
+    for r in reqs:
+        start = max(t_free, r.arrival)
+        t_free = start + alone_mean / 1e3
+        seq_lat.append((t_free - r.arrival) * 1e3)
+
+    # end to end: the first 200 requests with host-side initial fields
+    # (copied in at admission) and every result read back to the host
+    e2e_reqs = _serve_workload(200, seed=4 + rank, host_init=True)
+    for r in e2e_reqs:
+        r.init = tuple(torch.from_numpy(a).pin_memory() for a in r.init)
+    h2d = sum(a.numel() * a.element_size() for r in e2e_reqs for a in r.init)
+    host_out = [tuple(torch.empty(r.shape, dtype=getattr(torch, r.dtype), pin_memory=True)
+                      for _ in range(D.SERVE_KINDS[r.kind][2])) for r in e2e_reqs]
+    t0 = time.perf_counter()
+    eres = server.run(e2e_reqs, realtime=True, keep_state=True)
+    for r, o in zip(eres, host_out):
+        for dst, src in zip(o, r.state):
+            dst.copy_(src, non_blocking=True)
+    torch.cuda.synchronize()
+    e2e_span = time.perf_counter() - t0
+    d2h = sum(t.numel() * t.element_size() for o in host_out for t in o)
+    del eres, host_out
+
+    line = {
+        "metric": SERVE_METRIC, "value": round(solves_s, 3), "unit": "solves/s",
+        "n_gpus": world, "steps": len(reqs), "warmup": args.warmup,
+        "ms_per_step": round(span * 1e3 / len(reqs), 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32/f64 mix", "data": "synthetic",
+        "config": {"workload": f"{len(reqs)} requests, Poisson arrivals at {SERVE_RATE:.0f}/s "
+                               f"(seed 4): heat 5-pt, upwind advection (1, 0.5), leapfrog wave "
+                               f"c=1, 3-D 7-pt; 2-D N log-uniform 64..4096, 3-D 32..256; steps "
+                               f"log-uniform 10..1000; float32/float64 50/50; Uniform[0,1) "
+                               f"interiors generated on the device; zero Dirichlet halo; "
+                               f"HBM admission budget {SERVE_BUDGET / 1e9:.0f} GB; a step is one "
+                               f"request",
+                   "l2": "working set >> 126 MB L2",
+                   "parallelism": f"replicas{world}"},
+        "latency_ms": {"p50": round(percentile(lat, 50), 3), "p99": round(percentile(lat, 99), 3),
+                       "mean": round(float(np.mean(lat)), 3)},
+        "comparison": {
+            "alone_plain_solves_s": round(1e3 / alone_mean, 3),
+            "speedup_vs_alone_plain": round(solves_s / (1e3 / alone_mean), 3),
+            "alone_sequential_latency_ms": {"p50": round(percentile(seq_lat, 50), 3),
+                                            "p99": round(percentile(seq_lat, 99), 3)},
+            "alone": f"each request by itself, one launch_<name> per step on C-contiguous "
+                     f"fields, device time of {len(sample)} sampled requests (mean "
+                     f"{alone_mean:.3f} ms); sequential latencies assume FIFO on one GPU",
+            "gpts_served": round(gpts, 3),
+            "server": {"iterations": st.iterations, "launches": st.launches,
+                       "max_active": st.max_active, "peak_gb": round(st.peak_bytes / 1e9, 3),
+                       "rejected": st.rejected, "wall_s": round(st.wall, 3)},
+        },
+        "roofline": None,
+        "e2e": {"value": round(len(e2e_reqs) / e2e_span, 3), "unit": "solves/s",
+                "h2d_bytes_per_step": int(h2d / len(e2e_reqs)),
+                "d2h_bytes_per_step": int(d2h / len(e2e_reqs)),
+                "step": "one request: pinned host fields copied in at admission, result read "
+                        "back after the run (first 200 requests of the stream)"},
+        "gpu_launches": st.launches,
+        "clocks": clocks,
+        "cpu_baseline": None,
+    }
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return line if rank == 0 else None
+
+
 def run_sw_reference(args) -> dict | None:
     world, rank, _ = _dist()
     if rank != 0:
@@ -882,7 +1057,10 @@ def main() -> None:
     ap.add_argument("--temporal", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--n", type=int, default=512, help="interior extent per dimension")
-    ap.add_argument("--workload", choices=("lap7", "sw_batch", "gray_scott"), default="lap7",
+    ap.add_argument("--serve-requests", type=int, default=2000,
+                    help="serve: number of requests in the stream")
+    ap.add_argument("--workload", choices=("lap7", "sw_batch", "gray_scott", "serve"),
+                    default="lap7",
                     help="lap7: 3-D 7-point 512^3 sweeps; sw_batch: 256 batched shallow-water "
                          "solves; gray_scott: 4096^2 fused Gray-Scott, FP64/FP32/Kahan")
     ap.add_argument("--sw-grids", type=int, default=256, help="sw_batch: number of grids")
@@ -901,9 +1079,17 @@ def main() -> None:
     N_INTERIOR = args.n
     SW_GRIDS, SW_FIXED_N, SW_STEPS = args.sw_grids, args.sw_n, args.sw_steps
     SW_ZCHUNK = args.sw_zchunk
+    global SERVE_REQUESTS
+    SERVE_REQUESTS = args.serve_requests
     if args.warmup < 3:
         args.warmup = 3
-    if args.workload == "gray_scott":
+    if args.workload == "serve":
+        if args.impl == "reference":
+            line = {"impl": "reference", "unavailable": "the reference has no serving layer "
+                    "(one launch per grid); the plain-path comparison is in the serve line"}
+        else:
+            line = run_serve(args)
+    elif args.workload == "gray_scott":
         if args.steps_given is None:
             args.steps = GS_STEPS if args.impl == "ours" else 3
         line = run_gs_reference(args) if args.impl == "reference" else run_gray_scott(args)

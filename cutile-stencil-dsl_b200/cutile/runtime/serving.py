@@ -1,0 +1,350 @@
+"""Continuous-batching stencil solve server (device-resident, HBM-admitted).
+
+A *solve* is one request: a stencil kind, a dtype, an initial state and a
+step count.  The server keeps every admitted solve's fields resident on the
+device and advances all of them together, one time step per *iteration*:
+each (kind, dtype) group of active solves is one persistent batched launch
+over a device work list (``csd_launch_batch``), so many small grids share a
+launch and large ones stream beside them.  Solves that arrive while others
+are running are admitted at the next iteration boundary, first come first
+served, as long as their fields fit the HBM budget; a finished solve frees
+its memory at the iteration that completes it.  That is iteration-level
+(continuous) batching: nothing waits for a whole batch to drain.
+
+The reference has no serving layer (it launches one grid per call,
+``launch_<name>`` in target_to_python.py:305-348); every kernel here is the
+same stencil kernel a single launch runs, so a solve's result is bit-identical
+alone and in the mix.
+
+State rotation: a kind with ``nstate`` state fields (1 for a plain update,
+2 for a leapfrog ``u_new = f(u, u_prev)``) keeps ``nstate + 1`` buffers; at
+phase p the state is ``bufs[p], bufs[p-1], ...`` (newest first) and the step
+writes ``bufs[p+1]`` (indices mod ``nstate + 1``).  Buffers are allocated
+zeroed, so a zero Dirichlet halo stays zero (kernels write interiors only).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+from cutile.runtime import native
+
+
+@dataclass
+class SolveKind:
+    """A stencil kind the server can run: compiled results per dtype
+    (``{"float32": CompileResult, "float64": CompileResult}``), each taking
+    ``nstate`` input fields and producing one output field."""
+
+    name: str
+    results: dict
+    nstate: int = 1
+
+
+@dataclass
+class SolveRequest:
+    kind: str
+    dtype: str                 # "float32" or "float64"
+    shape: tuple               # array shape, halo included
+    steps: int
+    arrival: float = 0.0       # seconds after the server starts
+    init: object = None        # tuple of state arrays (newest first) or None
+    seed: int = 0              # device Uniform[0,1) interior when init is None
+    rid: int = -1
+
+
+@dataclass
+class SolveResult:
+    rid: int
+    kind: str
+    dtype: str
+    shape: tuple
+    steps: int
+    arrival: float
+    admitted: float = math.nan
+    completed: float = math.nan
+    state: tuple = ()          # device tensors, newest first (interior + zero halo)
+    error: str | None = None
+
+    @property
+    def latency(self) -> float:
+        return self.completed - self.arrival
+
+
+@dataclass
+class _Active:
+    req: SolveRequest
+    res: SolveResult
+    flat: object
+    bufs: list
+    desc: object               # numpy uint8 [phases, grid_size]
+    items: int
+    phase: int = 0
+    done: int = 0
+    nbytes: int = 0
+
+
+@dataclass
+class ServerStats:
+    iterations: int = 0
+    launches: int = 0
+    peak_bytes: int = 0
+    max_active: int = 0
+    admitted: int = 0
+    rejected: int = 0
+    wall: float = 0.0
+    trace: list = field(default_factory=list)   # (time, active, used_bytes) per iteration
+
+
+def percentile(values, q: float) -> float:
+    """Nearest-rank percentile (q in [0, 100]) of a non-empty sequence."""
+    v = sorted(values)
+    if not v:
+        return math.nan
+    k = max(0, min(len(v) - 1, math.ceil(q / 100.0 * len(v)) - 1))
+    return v[k]
+
+
+def batch_zchunk(kernel: native.NativeKernel) -> int:
+    """Rows per work item in a batched launch: short items for issue-bound
+    bodies (kernels whose default asks for several items per resident
+    block), long ones for memory-bound bodies."""
+    d = kernel.desc
+    return 2 * d["rows"] if d["zchunk"] < 0 else 64
+
+
+class StencilServer:
+    """Run solve requests with continuous batching under an HBM budget."""
+
+    def __init__(self, kinds, budget_bytes: float = 150e9, device=None):
+        import torch
+
+        self.kinds = {k.name: k for k in kinds}
+        self.budget = int(budget_bytes)
+        if device is None:
+            device = torch.device("cuda", torch.cuda.current_device())
+        self.device = torch.device(device)
+        self._progs: dict = {}
+        self._dev_desc: dict = {}
+        self.stats = ServerStats()
+
+    # -- programs ----------------------------------------------------------
+    def program(self, kind: str, dtype: str):
+        key = (kind, dtype)
+        p = self._progs.get(key)
+        if p is None:
+            k = self.kinds[kind]
+            if dtype not in k.results:
+                raise KeyError(f"kind {kind!r} has no {dtype} program")
+            prog = k.results[dtype].load_module().program()
+            if prog.spec["inputs"] != k.nstate or prog.spec["outputs"] != 1:
+                raise ValueError(f"kind {kind!r}: the stencil must read {k.nstate} field(s) and "
+                                 f"write one")
+            kern = prog.kernel("main")
+            p = (prog, kern, batch_zchunk(kern))
+            self._progs[key] = p
+        return p
+
+    def memory_of(self, req: SolveRequest) -> int:
+        """Device bytes a request holds while active (its rotating buffers,
+        rows padded to 128 bytes)."""
+        esz = 8 if req.dtype == "float64" else 4
+        per_row = -(-req.shape[-1] * esz // 128) * 128
+        outer = 1
+        for x in req.shape[:-1]:
+            outer *= x
+        span = -(-outer * per_row // 256) * 256
+        return (self.kinds[req.kind].nstate + 1) * span
+
+    # -- admission ---------------------------------------------------------
+    def _admit(self, req: SolveRequest, res: SolveResult, now: float) -> _Active:
+        import numpy as np
+        import torch
+
+        from cutile.runtime.rk_runtime import pack_grids
+
+        kind = self.kinds[req.kind]
+        prog, kern, zc = self.program(req.kind, req.dtype)
+        tdt = torch.float64 if req.dtype == "float64" else torch.float32
+        P = kind.nstate + 1
+        flat, (bufs,) = pack_grids([req.shape], P, tdt, self.device)
+        bufs = list(bufs)
+        halo = prog.spec["halo"]
+        inner = tuple(slice(h, s - h) for h, s in zip(halo, req.shape))
+        if req.init is not None:
+            init = tuple(req.init)
+            if len(init) != kind.nstate:
+                raise ValueError(f"request {req.rid}: {kind.nstate} initial field(s) expected")
+            for k, a in enumerate(init):
+                t = a if isinstance(a, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(a))
+                bufs[(-k) % P].copy_(t.to(device=self.device, dtype=tdt), non_blocking=True)
+        else:
+            g = torch.Generator(device=self.device)
+            g.manual_seed(int(req.seed))
+            interior = tuple(s - 2 * h for h, s in zip(halo, req.shape))
+            u = torch.rand(interior, generator=g, device=self.device, dtype=tdt)
+            for k in range(kind.nstate):
+                bufs[(-k) % P][inner].copy_(u)
+        gsz = native.grid_size()
+        desc = np.zeros((P, gsz), dtype=np.uint8)
+        items = 0
+        for p in range(P):
+            ins = [bufs[(p - k) % P] for k in range(kind.nstate)]
+            out = [bufs[(p + 1) % P]]
+            items, loader = native.grid_build(kern, ins, out, halo, desc[p].ctypes.data,
+                                              zchunk=zc, loader=native.CSD_LOADER_TMA)
+        res.admitted = now
+        return _Active(req=req, res=res, flat=flat, bufs=bufs, desc=desc, items=items,
+                       nbytes=flat.numel() * flat.element_size())
+
+    # -- one iteration -----------------------------------------------------
+    def _iterate(self, active: list, stream) -> None:
+        import numpy as np
+        import torch
+
+        groups: dict = {}
+        for a in active:
+            groups.setdefault((a.req.kind, a.req.dtype), []).append(a)
+        gsz = native.grid_size()
+        for key, members in groups.items():
+            prog, kern, zc = self.program(*key)
+            n = len(members)
+            host = np.concatenate([a.desc[a.phase] for a in members])
+            starts = np.zeros(n + 1, dtype=np.int32)
+            np.cumsum([a.items for a in members], out=starts[1:])
+            buf = self._dev_desc.get(key)
+            if buf is None or buf[0].numel() < host.size or buf[1].numel() < n + 1:
+                cap = max(host.size, 64 * gsz) * 2
+                buf = (torch.empty(cap, dtype=torch.uint8, device=self.device),
+                       torch.empty(2 * (n + 1) + 64, dtype=torch.int32, device=self.device))
+                self._dev_desc[key] = buf
+            # the previous iteration's launch has finished (host sync), so the
+            # device work list can be overwritten
+            buf[0][:host.size].copy_(torch.from_numpy(host), non_blocking=False)
+            buf[1][:n + 1].copy_(torch.from_numpy(starts), non_blocking=False)
+            native.launch_batch(kern, buf[0].data_ptr(), buf[1].data_ptr(), n, int(starts[-1]),
+                                stream, loader=native.CSD_LOADER_TMA)
+            self.stats.launches += 1
+
+    def _stream(self):
+        import torch
+
+        return torch.cuda.current_stream(self.device)
+
+    def _sync(self, stream) -> None:
+        stream.synchronize()
+
+    # -- the request loop --------------------------------------------------
+    def run(self, requests, *, realtime: bool = True, keep_state=True):
+        """Serve ``requests`` (any order; admitted by arrival, FIFO) and
+        return their results in request order.  ``realtime``: a request is
+        admissible only once the wall clock passes its arrival time.
+        ``keep_state``: True, False or a set of request ids whose final
+        fields the results keep (kept fields stay allocated after the budget
+        has released them)."""
+        reqs = list(requests)
+        for i, r in enumerate(reqs):
+            if r.rid < 0:
+                r.rid = i
+        results = {r.rid: SolveResult(rid=r.rid, kind=r.kind, dtype=r.dtype, shape=tuple(r.shape),
+                                      steps=r.steps, arrival=r.arrival) for r in reqs}
+        queue = deque(sorted(reqs, key=lambda r: (r.arrival, r.rid)))
+        active: list[_Active] = []
+        used = 0
+        stream = self._stream()
+        t0 = time.perf_counter()
+        st = self.stats
+        while queue or active:
+            now = time.perf_counter() - t0
+            # admit arrived requests in order while they fit
+            while queue and (not realtime or queue[0].arrival <= now):
+                r = queue[0]
+                need = self.memory_of(r)
+                if need > self.budget:
+                    queue.popleft()
+                    results[r.rid].error = (f"needs {need} bytes, more than the "
+                                            f"{self.budget}-byte budget")
+                    st.rejected += 1
+                    continue
+                if used + need > self.budget:
+                    break                       # first come, first served
+                queue.popleft()
+                a = self._admit(r, results[r.rid], now)
+                active.append(a)
+                used += a.nbytes
+                st.admitted += 1
+            st.peak_bytes = max(st.peak_bytes, used)
+            st.max_active = max(st.max_active, len(active))
+            if not active:
+                if queue and realtime:
+                    time.sleep(max(0.0, min(queue[0].arrival - now, 0.01)))
+                continue
+            self._iterate(active, stream)
+            self._sync(stream)
+            now = time.perf_counter() - t0
+            st.iterations += 1
+            st.trace.append((now, len(active), used))
+            keep = []
+            for a in active:
+                a.done += 1
+                a.phase = (a.phase + 1) % len(a.bufs)
+                if a.done >= a.req.steps:
+                    res = a.res
+                    res.completed = now
+                    P = len(a.bufs)
+                    nstate = self.kinds[a.req.kind].nstate
+                    if keep_state is True or (keep_state and a.req.rid in keep_state):
+                        res.state = tuple(a.bufs[(a.phase - k) % P] for k in range(nstate))
+                    used -= a.nbytes
+                else:
+                    keep.append(a)
+            active = keep
+        st.wall = time.perf_counter() - t0
+        return [results[r.rid] for r in reqs]
+
+    # -- the plain path --------------------------------------------------------
+    def run_alone(self, req: SolveRequest):
+        """One request by itself through the drop-in launch (one
+        ``launch_<name>`` per step on C-contiguous fields): returns
+        ``(state, device_ms)``."""
+        import numpy as np
+        import torch
+
+        kind = self.kinds[req.kind]
+        prog, _kern, _zc = self.program(req.kind, req.dtype)
+        tdt = torch.float64 if req.dtype == "float64" else torch.float32
+        P = kind.nstate + 1
+        bufs = [torch.zeros(req.shape, dtype=tdt, device=self.device) for _ in range(P)]
+        halo = prog.spec["halo"]
+        inner = tuple(slice(h, s - h) for h, s in zip(halo, req.shape))
+        if req.init is not None:
+            for k, a in enumerate(req.init):
+                t = a if isinstance(a, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(a))
+                bufs[(-k) % P].copy_(t.to(device=self.device, dtype=tdt))
+        else:
+            g = torch.Generator(device=self.device)
+            g.manual_seed(int(req.seed))
+            interior = tuple(s - 2 * h for h, s in zip(halo, req.shape))
+            u = torch.rand(interior, generator=g, device=self.device, dtype=tdt)
+            for k in range(kind.nstate):
+                bufs[(-k) % P][inner].copy_(u)
+        stream = torch.cuda.current_stream(self.device)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for s in range(req.steps):
+            p = s % P
+            prog.launch([bufs[(p - k) % P] for k in range(kind.nstate)], [bufs[(p + 1) % P]],
+                        stream)
+        e1.record(stream)
+        e1.synchronize()
+        p = req.steps % P
+        return tuple(bufs[(p - k) % P] for k in range(kind.nstate)), e0.elapsed_time(e1)
+
+
+__all__ = ["SolveKind", "SolveRequest", "SolveResult", "StencilServer", "ServerStats",
+           "percentile", "batch_zchunk"]

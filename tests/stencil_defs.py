@@ -205,3 +205,29 @@ def sw_init(n: int, rng, halo=(1, 1), dtype="float32"):
     h[halo[0]:halo[0] + n, halo[1]:halo[1] + n] = 1.0 + 0.1 * np.exp(-r2 / (2 * 0.05 ** 2))
     z = np.zeros(shape)
     return h.astype(dtype), z.astype(dtype), z.astype(dtype)
+
+
+# Serving mix: 2-D heat 5-pt, 2-D first-order upwind advection with velocity
+# (1, 0.5) at Courant number 0.4 in x, 2-D leapfrog wave (c = 1, Courant^2
+# 0.25, state u, u_prev) and the 3-D 7-point Laplacian.
+def upwind2d(u, i, j):
+    return u[i, j] - 0.4 * (u[i, j] - u[i, j - 1]) - 0.2 * (u[i, j] - u[i - 1, j])
+
+
+SERVE_KINDS = {"heat2d": (heat2d, 2, 1), "upwind2d": (upwind2d, 2, 1),
+               "wave2d": (leapfrog, 2, 2), "lap7": (lap7, 3, 1)}
+
+
+def serving_kinds(align_halo: bool = False):
+    """SolveKind objects (FP32 and FP64 programs) for the serving mix."""
+    from cutile import compile as stencil_compile
+    from cutile import stencil
+    from cutile.runtime.serving import SolveKind
+
+    kinds = []
+    for name, (fn, ndim, nstate) in SERVE_KINDS.items():
+        res = {dt: stencil_compile(stencil(ndim=ndim, dtype=dt)(fn), temporal_blocking=False,
+                                   align_halo=align_halo)
+               for dt in ("float32", "float64")}
+        kinds.append(SolveKind(name, res, nstate))
+    return kinds
