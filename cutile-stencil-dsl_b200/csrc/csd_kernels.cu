@@ -129,6 +129,143 @@ extern "C" int csd_apply_boundary(const csd_field* f, const int* halo, int bc, d
 }
 
 // ---------------------------------------------------------------------------
+// Bricked layout conversions
+//
+// A bricked array holds a (n0, n1, n2) array (1-3 dims, leading dims 1) as
+// bricks of B^nd elements, bricks in row-major order over the brick grid
+// (ceil(n / B) per dim) and each brick row-major inside: the reference's
+// to_bricks reshape/transpose (multigpu_emitter.py:370-408), padded cells
+// zero.  One thread per element; to_bricks walks the bricked order (writes
+// coalesced, reads in runs of B), from_bricks the flat order.
+// ---------------------------------------------------------------------------
+namespace {
+
+__device__ __forceinline__ long long brick_off(long long z, long long y, long long x, int nd, int s,
+                                               long long nby, long long nbx) {
+  const long long m = (1ll << s) - 1;
+  if (nd == 3)
+    return ((((z >> s) * nby + (y >> s)) * nbx + (x >> s)) << (3 * s)) + ((z & m) << (2 * s)) +
+           ((y & m) << s) + (x & m);
+  if (nd == 2) return ((((y >> s) * nbx + (x >> s)) << (2 * s)) + ((y & m) << s) + (x & m));
+  return x;
+}
+
+template <typename T>
+__global__ void to_bricks_kernel(const T* __restrict__ flat, T* __restrict__ bricked, long long n0,
+                                 long long n1, long long n2, int nd, int s, long long nb0,
+                                 long long nb1, long long nb2) {
+  const long long B = 1ll << s;
+  const long long total = nb0 * nb1 * nb2 * (nd == 3 ? B * B * B : nd == 2 ? B * B : B);
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    long long z = 0, y = 0, x;
+    const long long m = B - 1;
+    if (nd == 3) {
+      const long long b = e >> (3 * s), r = e & ((1ll << (3 * s)) - 1);
+      x = ((b % nb2) << s) + (r & m);
+      y = (((b / nb2) % nb1) << s) + ((r >> s) & m);
+      z = ((b / (nb2 * nb1)) << s) + (r >> (2 * s));
+    } else if (nd == 2) {
+      const long long b = e >> (2 * s), r = e & ((1ll << (2 * s)) - 1);
+      x = ((b % nb2) << s) + (r & m);
+      y = ((b / nb2) << s) + (r >> s);
+    } else {
+      x = e;
+    }
+    const bool in = z < n0 && y < n1 && x < n2;
+    bricked[e] = in ? flat[(z * n1 + y) * n2 + x] : T(0);
+  }
+}
+
+template <typename T>
+__global__ void from_bricks_kernel(const T* __restrict__ bricked, T* __restrict__ flat, long long n0,
+                                   long long n1, long long n2, int nd, int s, long long nb1,
+                                   long long nb2) {
+  const long long total = n0 * n1 * n2;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long x = e % n2, t = e / n2, y = t % n1, z = t / n1;
+    flat[e] = bricked[brick_off(z, y, x, nd, s, nb1, nb2)];
+  }
+}
+
+// (n0, n1, n2) view, bricked dimensionality and brick-grid extents of a field
+int brick_geometry(const csd_field* f, int brick, long long n[3], long long nb[3], int* nd,
+                   int* s) {
+  if (!f || !f->ptr) return csd_internal_fail(CSD_EINVAL, "null field");
+  if (f->ndim < 1 || f->ndim > 3) return csd_internal_fail(CSD_EINVAL, "ndim must be 1-3");
+  if (brick < 2 || brick > 1024 || (brick & (brick - 1)))
+    return csd_internal_fail(CSD_EINVAL, "brick size must be a power of two in [2, 1024]");
+  if (!packed(f)) return csd_internal_fail(CSD_EINVAL, "the flat array must be C-contiguous");
+  *nd = f->ndim;
+  *s = 0;
+  while ((1 << *s) < brick) ++*s;
+  const int off = 3 - f->ndim;
+  for (int i = 0; i < 3; ++i) n[i] = 1;
+  for (int i = 0; i < f->ndim; ++i) n[off + i] = f->shape[i];
+  for (int i = 0; i < 3; ++i) nb[i] = (i < off) ? 1 : (n[i] + brick - 1) / brick;
+  return CSD_OK;
+}
+
+}  // namespace
+
+extern "C" long long csd_bricked_elems(const long long* shape, int ndim, int brick) {
+  if (!shape || ndim < 1 || ndim > 3 || brick < 1) return -1;
+  long long e = 1;
+  for (int i = 0; i < ndim; ++i) e *= ((shape[i] + brick - 1) / brick) * brick;
+  return e;
+}
+
+extern "C" int csd_to_bricks(const csd_field* flat, int brick, void* bricked, void* stream) {
+  long long n[3], nb[3];
+  int nd = 0, s = 0;
+  int rc = brick_geometry(flat, brick, n, nb, &nd, &s);
+  if (rc) return rc;
+  if (!bricked) return csd_internal_fail(CSD_EINVAL, "null bricked buffer");
+  const long long total = nb[0] * nb[1] * nb[2] * (nd == 3 ? (long long)brick * brick * brick
+                                                   : nd == 2 ? (long long)brick * brick : brick);
+  long long blocks = (total + 255) / 256;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  if (flat->dtype == CSD_DTYPE_F64)
+    to_bricks_kernel<double><<<(int)blocks, 256, 0, st>>>(
+        static_cast<const double*>(flat->ptr), static_cast<double*>(bricked), n[0], n[1], n[2], nd,
+        s, nb[0], nb[1], nb[2]);
+  else if (flat->dtype == CSD_DTYPE_F32)
+    to_bricks_kernel<float><<<(int)blocks, 256, 0, st>>>(
+        static_cast<const float*>(flat->ptr), static_cast<float*>(bricked), n[0], n[1], n[2], nd,
+        s, nb[0], nb[1], nb[2]);
+  else
+    return csd_internal_fail(CSD_EINVAL, "unsupported dtype");
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? CSD_OK : csd_internal_fail(CSD_ELAUNCH, cudaGetErrorString(e));
+}
+
+extern "C" int csd_from_bricks(const void* bricked, int brick, const csd_field* flat, void* stream) {
+  long long n[3], nb[3];
+  int nd = 0, s = 0;
+  int rc = brick_geometry(flat, brick, n, nb, &nd, &s);
+  if (rc) return rc;
+  if (!bricked) return csd_internal_fail(CSD_EINVAL, "null bricked buffer");
+  const long long total = n[0] * n[1] * n[2];
+  long long blocks = (total + 255) / 256;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  if (flat->dtype == CSD_DTYPE_F64)
+    from_bricks_kernel<double><<<(int)blocks, 256, 0, st>>>(
+        static_cast<const double*>(bricked), static_cast<double*>(flat->ptr), n[0], n[1], n[2], nd,
+        s, nb[1], nb[2]);
+  else if (flat->dtype == CSD_DTYPE_F32)
+    from_bricks_kernel<float><<<(int)blocks, 256, 0, st>>>(
+        static_cast<const float*>(bricked), static_cast<float*>(flat->ptr), n[0], n[1], n[2], nd,
+        s, nb[1], nb[2]);
+  else
+    return csd_internal_fail(CSD_EINVAL, "unsupported dtype");
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? CSD_OK : csd_internal_fail(CSD_ELAUNCH, cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------------------
 // FP64 reductions over the interior of a field (mass, energy, residual, max)
 //
 // Deterministic: pass 1 gives CTA b the interior rows [b*R/G, (b+1)*R/G) of

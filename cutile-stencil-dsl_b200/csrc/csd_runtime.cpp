@@ -490,7 +490,8 @@ static int build_grid(csd_kernel* k, const csd_field* in, int n_in, const csd_fi
     for (int d = 0; d < f.ndim; ++d)
       if (f.shape[d] != f0.shape[d]) return fail(CSD_EINVAL, "all fields must have the same shape");
     if (f.dtype != want_dtype) return fail(CSD_EINVAL, "field dtype does not match the kernel");
-    if (!row_pitched(f)) return fail(CSD_EINVAL, "fields must be C-contiguous or row-pitched");
+    if (D.brick_shift == 0 && !row_pitched(f))
+      return fail(CSD_EINVAL, "fields must be C-contiguous or row-pitched");
     for (int d = 0; d < f.ndim; ++d)
       if (f.shape[d] != 1 && f.strides[d] != f0.strides[d])
         return fail(CSD_EINVAL, "all fields of a grid must have the same strides");
@@ -531,8 +532,19 @@ static int build_grid(csd_kernel* k, const csd_field* in, int n_in, const csd_fi
   g->tiles[0] = (g->halo[2] + g->interior[2] - g->xbase + D.tile_x - 1) / D.tile_x;
   g->tiles[1] = (g->interior[1] + D.tile_y - 1) / D.tile_y;
   const long long esz = D.dtype_bytes;
+  if (D.brick_shift > 0) {
+    // bricked fields: the shape is the logical (padded-array) shape; bricks
+    // of B^ndim elements cover it rounded up to whole bricks
+    const long long B = 1ll << D.brick_shift;
+    g->brick_shift = D.brick_shift;
+    g->nbx = (int)((g->dims[2] + B - 1) / B);
+    g->nby = f0.ndim == 3 ? (int)((g->dims[1] + B - 1) / B) : 1;
+    if (o.loader == CSD_LOADER_TMA)
+      return fail(CSD_EINVAL, "bricked fields are staged with the cp.async loader");
+  }
   // Loader: TMA when every input is 16-byte aligned with 16-byte pitches.
-  bool tma_ok = ((g->pitch_y * esz) % 16 == 0) && ((g->pitch_z * esz) % 16 == 0);
+  bool tma_ok = D.brick_shift == 0 && ((g->pitch_y * esz) % 16 == 0) &&
+                ((g->pitch_z * esz) % 16 == 0);
   for (int i = 0; i < n_in; ++i) tma_ok = tma_ok && (reinterpret_cast<uintptr_t>(in[i].ptr) % 16 == 0);
   int loader = loader_req;
   if (loader < 0 || loader > 1) loader = tma_ok ? CSD_LOADER_TMA : CSD_LOADER_LDG;
@@ -566,7 +578,7 @@ static int build_grid(csd_kernel* k, const csd_field* in, int n_in, const csd_fi
   g->red = o.red;
   bool vec = true;
   for (int i = 0; i < n_out; ++i) vec = vec && (reinterpret_cast<uintptr_t>(out[i].ptr) % 16 == 0);
-  vec = vec && ((g->pitch_y * esz) % 16 == 0) && ((g->pitch_z * esz) % 16 == 0);
+  if (D.brick_shift == 0) vec = vec && ((g->pitch_y * esz) % 16 == 0) && ((g->pitch_z * esz) % 16 == 0);
   g->vec_store = vec ? 1 : 0;
   if (loader == CSD_LOADER_TMA) {
     Driver& d = drv();

@@ -51,9 +51,13 @@ __host__ __device__ constexpr int imax(int a, int b) { return a > b ? a : b; }
 // Compile-time configuration
 // ---------------------------------------------------------------------------
 template <typename T_, int NIN_, int NOUT_, int RZ_, int RY_, int RX_, int ROWS_, int TY_, int TX_,
-          int NT_, int STAGES_, int TEMPORAL_, int LOADER_, int BC_, int REDUCE_ = 0>
+          int NT_, int STAGES_, int TEMPORAL_, int LOADER_, int BC_, int REDUCE_ = 0,
+          int BRICK_ = 0>
 struct Cfg {
   typedef T_ T;
+  // Bricked layout: BRICK_ = (ndim << 4) | log2(brick size), 0 = flat.
+  static constexpr int BRICK_SHIFT = BRICK_ & 15, BRICK_NDIM = BRICK_ >> 4;
+  static_assert(BRICK_ == 0 || LOADER_ == CSD_LOADER_LDG, "bricked fields use the cp.async loader");
   static constexpr int NIN = NIN_, NOUT = NOUT_;
   static constexpr int RZ = RZ_, RY = RY_, RX = RX_;  // radius of ONE step
   static constexpr int ROWS = ROWS_, TY = TY_, TX = TX_;
@@ -226,6 +230,28 @@ __device__ __forceinline__ double sqrt_rn(double x) {
   return z ? x : r;
 }
 
+// Element offset of array cell (z, y, x) (internal 3-D view): pitched rows,
+// or bricks of B^ndim elements (brick-major, row-major inside a brick).
+template <class C>
+__device__ __forceinline__ long long elem_off(const csd_grid& g, long long z, long long y,
+                                              long long x) {
+  if constexpr (C::BRICK_SHIFT == 0) {
+    return z * g.pitch_z + y * g.pitch_y + x;
+  } else {
+    constexpr int S = C::BRICK_SHIFT;
+    constexpr long long M = (1ll << S) - 1;
+    if constexpr (C::BRICK_NDIM == 3) {
+      const long long b = ((z >> S) * g.nby + (y >> S)) * g.nbx + (x >> S);
+      return (b << (3 * S)) + ((z & M) << (2 * S)) + ((y & M) << S) + (x & M);
+    } else if constexpr (C::BRICK_NDIM == 2) {
+      const long long b = (z >> S) * g.nbx + (x >> S);
+      return (b << (2 * S)) + ((z & M) << S) + (x & M);
+    } else {
+      return x;  // 1-D bricks are contiguous runs: the flat layout
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Chunk loaders
 // ---------------------------------------------------------------------------
@@ -292,7 +318,7 @@ struct Loader {
         const int rr = t / C::BOXH;
         const long long gx = (long long)x0 + xx, gy = (long long)y0 + yy, gz = (long long)z0 + rr;
         const bool ok = gx >= 0 && gx < NX && gy >= 0 && gy < NY && gz >= 0 && gz < NZ;
-        const long long off = ok ? (gz * g.pitch_z + gy * g.pitch_y + gx) : 0;
+        const long long off = ok ? elem_off<C>(g, gz, gy, gx) : 0;
 #pragma unroll
         for (int f = 0; f < C::NIN; ++f) {
           T* dst = ring + (f * C::NSLOT + slot) * C::SLOT_ELEMS + e;
@@ -341,7 +367,7 @@ __device__ __forceinline__ void patch_cell(const csd_grid& g, typename C::T* rin
       const long long mx = out_x ? bc_map(gx, hx, nx, C::BC) : gx;
       const long long my = out_y ? bc_map(gy, hy, ny, C::BC) : gy;
       const long long mz = out_z ? bc_map(gz, hz, nz, C::BC) : gz;
-      v = reinterpret_cast<const T*>(g.in[f])[mz * g.pitch_z + my * g.pitch_y + mx];
+      v = reinterpret_cast<const T*>(g.in[f])[elem_off<C>(g, mz, my, mx)];
       if (C::BC == CSD_BC_REFLECTING && odd_flip<C>(g, f, out_x, out_y, out_z)) v = -v;
     }
     ring[(f * C::NSLOT + slot) * C::SLOT_ELEMS + e] = v;
@@ -624,18 +650,35 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
               }
               continue;
             }
-            const long long rowoff = (long long)gz * pitch_z + (long long)gy * pitch_y;
             const bool full = gx0 >= hx && gx0 + C::VEC <= hx + nx;
+            if constexpr (C::BRICK_SHIFT == 0) {
+              const long long rowoff = (long long)gz * pitch_z + (long long)gy * pitch_y;
 #pragma unroll
-            for (int f = 0; f < C::NOUT; ++f) {
-              T* out = outp[f] + rowoff;
-              if (full && vec_store) {
-                store_vec(out + gx0, o.v[f]);
-              } else {
+              for (int f = 0; f < C::NOUT; ++f) {
+                T* out = outp[f] + rowoff;
+                if (full && vec_store) {
+                  store_vec(out + gx0, o.v[f]);
+                } else {
 #pragma unroll
-                for (int e = 0; e < C::VEC; ++e) {
-                  const int gx = gx0 + e;
-                  if (gx >= hx && gx < hx + nx) out[gx] = o.v[f][e];
+                  for (int e = 0; e < C::VEC; ++e) {
+                    const int gx = gx0 + e;
+                    if (gx >= hx && gx < hx + nx) out[gx] = o.v[f][e];
+                  }
+                }
+              }
+            } else {
+              // a VEC-aligned run of VEC points stays inside one brick row
+              const long long off0 = elem_off<C>(g, gz, gy, gx0);
+#pragma unroll
+              for (int f = 0; f < C::NOUT; ++f) {
+                if (full && vec_store) {
+                  store_vec(outp[f] + off0, o.v[f]);
+                } else {
+#pragma unroll
+                  for (int e = 0; e < C::VEC; ++e) {
+                    const int gx = gx0 + e;
+                    if (gx >= hx && gx < hx + nx) outp[f][off0 + e] = o.v[f][e];
+                  }
                 }
               }
             }

@@ -51,6 +51,11 @@ typedef struct __attribute__((aligned(64))) csd_grid {
   double* red;                        // per-grid max-reduction slot, may be null
   double bc_value;                    // Dirichlet value of a fused boundary fill
   int bc_odd[CSD_MAX_FIELDS];         // bit d: mirrored values of field f flip sign in dim d
+  // Bricked fields (kernels compiled for a brick size): the array is stored
+  // as bricks of B^ndim elements (B = 1 << brick_shift), brick-major, each
+  // brick row-major inside; nbx / nby bricks along X / Y of the padded array.
+  int brick_shift;                    // 0: flat (pitched) layout
+  int nbx, nby;
 } csd_grid;
 
 // Kernel parameter: one grid inline, or a device array of grids.
@@ -90,6 +95,7 @@ typedef struct csd_kernel_desc {
   int nscalars;      // static per-grid scalars the body reads
   int ndyn;          // device per-grid scalars the body reads
   int reduce_max;    // 1: the body also max-reduces a value into grid.red
+  int brick_shift;   // log2 of the brick size of a bricked-layout kernel (0 = flat)
 } csd_kernel_desc;
 
 #ifdef __cplusplus

@@ -255,7 +255,18 @@ def engine_params(kernel: KernelOp) -> dict:
         "NSCAL": kernel.scalar_count.data if kernel.scalar_count is not None else 0,
         "NDYN": kernel.dyn_count.data if kernel.dyn_count is not None else 0,
         "REDUCE": kernel.reduce_max.data if kernel.reduce_max is not None else 0,
+        "BRICK": _brick_code(kernel, ndim),
     }
+
+
+def _brick_code(kernel: KernelOp, ndim: int) -> int:
+    """(ndim << 4) | log2(brick size) for a bricked-layout kernel, else 0."""
+    if kernel.layout is None or kernel.layout.data != "bricked":
+        return 0
+    b = kernel.brick_size.data if kernel.brick_size is not None else 0
+    if b < 4 or b > 64 or (b & (b - 1)):
+        raise ValueError(f"brick size must be a power of two in [4, 64], got {b}")
+    return (ndim << 4) | (b.bit_length() - 1)
 
 
 def emit_cuda(module: ModuleOp, preamble: bool = True) -> str:
@@ -283,9 +294,11 @@ def emit_cuda(module: ModuleOp, preamble: bool = True) -> str:
         parts.append(emit_body(kernel))
         parts.append("")
         for suffix, loader in (("tma", "CSD_LOADER_TMA"), ("ldg", "CSD_LOADER_LDG")):
+            if p["BRICK"]:
+                loader = "CSD_LOADER_LDG"   # bricked fields: both entries use cp.async
             cfg = (f"csd::Cfg<{p['T']}, {p['NIN']}, {p['NOUT']}, {p['RZ']}, {p['RY']}, {p['RX']}, "
                    f"{p['ROWS']}, {p['TY']}, {p['TX']}, {p['NT']}, {p['STAGES']}, {p['TEMPORAL']}, "
-                   f"{loader}, {p['BC']}, {p['REDUCE']}>")
+                   f"{loader}, {p['BC']}, {p['REDUCE']}, {p['BRICK']}>")
             parts.append(f"typedef {cfg} Cfg_{name}_{suffix};")
             parts.append(f'extern "C" __global__ void __launch_bounds__({p["NT"]}, {p["MINB"]})')
             parts.append(f"{name}_{suffix}(const __grid_constant__ csd_params p) {{")
@@ -299,7 +312,7 @@ def emit_cuda(module: ModuleOp, preamble: bool = True) -> str:
         parts.append(f"  {c}::ROWS, {c}::TY, {c}::TX, {c}::VEC, {c}::NT, {c}::STAGES, {c}::NSLOT,")
         parts.append(f"  {c}::HC * {c}::TEMPORAL, {c}::PADL, {c}::BOXW, {c}::BOXH, {c}::SMEM_BYTES,")
         parts.append(f"  {p['ZCHUNK']}, {c}::TEMPORAL, {c}::BC, {p['MINB']}, {c}::ALIGN,")
-        parts.append(f"  {p['NSCAL']}, {p['NDYN']}, {p['REDUCE']}}};")
+        parts.append(f"  {p['NSCAL']}, {p['NDYN']}, {p['REDUCE']}, {c}::BRICK_SHIFT}};")
         parts.append("")
     return "\n".join(parts) + "\n"
 

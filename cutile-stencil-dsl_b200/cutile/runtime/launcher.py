@@ -321,6 +321,37 @@ def generate_module_code(name: str, cuda_source: str, spec: dict, *, fused_outpu
         with e.indent():
             e.line('"""One step with the boundary condition fused into the staging."""')
             e.line(f"_PROGRAM.step(({', '.join(inputs)},), ({', '.join(outs)},), stream, scalars={sc})")
+    if spec.get("layout") == "bricked":
+        bs = spec["brick_size"]
+        e.blank()
+        e.blank()
+        e.line(f"def to_bricks(flat_array, brick_size={bs}, stream=None):")
+        with e.indent():
+            e.line('"""Bricked copy of a flat device array (one kernel launch)."""')
+            e.line("return _PROGRAM.to_bricks(flat_array, brick_size, stream)")
+        e.blank()
+        e.blank()
+        e.line(f"def from_bricks(bricked, original_shape, brick_size={bs}, stream=None):")
+        with e.indent():
+            e.line('"""Flat array of ``original_shape`` from its bricked form."""')
+            e.line("return _PROGRAM.from_bricks(bricked, original_shape, brick_size, stream)")
+        e.blank()
+        e.blank()
+        e.line(f"def launch_{name}_bricked({args}, brick_size={bs}, stream=None{kw}):")
+        with e.indent():
+            e.line('"""Bricked launch on flat arrays: the inputs are bricked, the bricked '
+                   'kernel runs, and')
+            e.line('the whole output is written back (interior = result, halo = 0)."""')
+            e.line(f"_PROGRAM.launch_bricked(({', '.join(inputs)},), ({', '.join(outs)},), "
+                   f"brick_size, stream, scalars={sc})")
+        e.blank()
+        e.blank()
+        e.line(f"def launch_{name}_on_bricks({args}, shape, stream=None{kw}):")
+        with e.indent():
+            e.line('"""The bricked kernel on fields already stored as bricks of a ``shape`` '
+                   'array."""')
+            e.line(f"_PROGRAM.launch_on_bricks(({', '.join(inputs)},), ({', '.join(outs)},), "
+                   f"shape, stream, scalars={sc})")
     e.blank()
     e.blank()
     e.line("def program():")
@@ -453,6 +484,14 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
         _rename_kernel(bc_target, f"{name}_bc")
         cuda += "\n" + emit_cuda(bc_target, preamble=False)
         kernels["fused_bc"] = f"{name}_bc"
+    if layout == "bricked":
+        # the same stencil reading and writing fields stored as bricks
+        bk_target = lower_to_target_ir(ir.clone(), plan.tile_sizes(), halo_widths,
+                                       temporal_steps=T, kernel_hints=hints, dtype=dtype,
+                                       kahan=kahan, layout="bricked", brick_size=int(brick_size))
+        _rename_kernel(bk_target, f"{name}_bk")
+        cuda += "\n" + emit_cuda(bk_target, preamble=False)
+        kernels["bricked"] = f"{name}_bk"
     in_names = _input_names(ir)
     n_fields = num_inputs - (1 if kahan else 0)
     multi = n_fields > 1
@@ -470,6 +509,7 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
         "input_names": names, "output_params": outs, "zchunk": plan.zchunk,
         "precision": precision or ("fp32" if dtype == "float32" else "fp64"),
         "scalars": _scalar_names(ir),
+        "layout": layout or "flat", "brick_size": int(brick_size) if layout == "bricked" else 0,
     }
     code = generate_module_code(name, cuda, spec)
     return CompileResult(

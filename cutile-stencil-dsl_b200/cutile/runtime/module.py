@@ -125,6 +125,63 @@ class StencilProgram:
                       scalars=self.scalar_values(scalars), red=out)
         return out
 
+    # -- bricked layout ------------------------------------------------------
+    def _brick(self, brick_size) -> int:
+        bs = int(brick_size)
+        if self.spec.get("layout") != "bricked" or "bricked" not in self.spec["kernels"]:
+            raise ValueError(f"{self.spec['name']} was not compiled with layout='bricked'")
+        if bs != self.spec["brick_size"]:
+            raise ValueError(f"{self.spec['name']}: compiled for brick size "
+                             f"{self.spec['brick_size']}, got {bs}")
+        return bs
+
+    def to_bricks(self, flat, brick_size, stream=None):
+        return native.to_bricks(flat, int(brick_size), stream)
+
+    def from_bricks(self, bricked, shape, brick_size, stream=None):
+        return native.from_bricks(bricked, shape, int(brick_size), stream=stream)
+
+    def launch_on_bricks(self, inputs, outputs, shape, stream=None, *,
+                         scalars: dict | None = None) -> None:
+        """The bricked kernel on bricked fields of a ``shape`` array: writes
+        the interior cells of the outputs' bricks (halo and padding cells
+        untouched)."""
+        bs = self._brick(self.spec["brick_size"])
+        shape = tuple(int(n) for n in shape)
+        if len(shape) != self.spec["ndim"]:
+            raise ValueError(f"{self.spec['name']}: expected a {self.spec['ndim']}-D shape")
+        if len(inputs) != self.spec["inputs"] or len(outputs) != self.spec["outputs"]:
+            raise TypeError(f"{self.spec['name']} takes {self.spec['inputs']} input(s) and "
+                            f"{self.spec['outputs']} output(s)")
+        for o in outputs:
+            for i in inputs:
+                if o.data_ptr() == i.data_ptr():
+                    raise ValueError("outputs must not alias inputs (the kernel reads neighbours)")
+        want = "float64" if self.spec["dtype"] in ("float64", "fp64") else "float32"
+        for t in list(inputs) + list(outputs):
+            if str(t.dtype).replace("torch.", "") != want:
+                raise TypeError(f"{self.spec['name']}: bricked field dtype {t.dtype} does not "
+                                f"match the compiled dtype {want}")
+        fin = [native.bricked_field(t, shape, bs) for t in inputs]
+        fout = [native.bricked_field(t, shape, bs) for t in outputs]
+        native.launch_fields(self.kernel("bricked"), fin, fout, self.spec["halo"], stream,
+                             loader=native.CSD_LOADER_LDG, scalars=self.scalar_values(scalars))
+
+    def launch_bricked(self, inputs, outputs, brick_size, stream=None, *,
+                       scalars: dict | None = None) -> None:
+        """``launch_<name>_bricked`` (multigpu_emitter.py:426-473): flat in,
+        flat out; every output is overwritten whole, interior with the
+        result and halo with zeros, as the reference's write-back of the
+        bricked result does."""
+        bs = self._brick(brick_size)
+        self._check(list(inputs) + list(outputs), "stencil")
+        shape = tuple(inputs[0].shape)
+        ins = [native.to_bricks(t.contiguous(), bs, stream) for t in inputs]
+        outs = [_zeros(native.bricked_shape(shape, bs), o) for o in outputs]
+        self.launch_on_bricks(ins, outs, shape, stream, scalars=scalars)
+        for o, ob in zip(outputs, outs):
+            native.from_bricks(ob, shape, bs, out=o, stream=stream)
+
     def apply_boundary(self, u, stream=None) -> None:
         """``apply_boundary_<name>(u)``: fill the halo of ``u`` in place."""
         bc = self.spec["boundary"]
@@ -133,6 +190,12 @@ class StencilProgram:
         self._check([u], "boundary")
         native.apply_boundary(u, self.spec["halo"], bc["type"], float(bc.get("value", 0.0)),
                               stream)
+
+
+def _zeros(shape, like):
+    import torch
+
+    return torch.zeros(tuple(shape), dtype=like.dtype, device=like.device)
 
 
 __all__ = ["StencilProgram"]

@@ -61,7 +61,7 @@ class KernelDesc(ctypes.Structure):
         "magic", "ndim", "nin", "nout", "dtype_bytes", "rz", "ry", "rx", "rows", "tile_y",
         "tile_x", "vec", "threads", "stages", "nslot", "halo_chunks", "pad_left", "box_w",
         "box_h", "smem_bytes", "zchunk", "temporal", "bc_mode", "min_blocks", "align",
-        "nscalars", "ndyn", "reduce_max")]
+        "nscalars", "ndyn", "reduce_max", "brick_shift")]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -102,6 +102,11 @@ def library() -> ctypes.CDLL:
         lib.csd_apply_boundary.argtypes = [ctypes.POINTER(Field), ctypes.POINTER(ctypes.c_int),
                                            ctypes.c_int, ctypes.c_double, P]
         lib.csd_error_word.argtypes = [ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+        lib.csd_bricked_elems.argtypes = [ctypes.POINTER(ctypes.c_longlong), ctypes.c_int,
+                                          ctypes.c_int]
+        lib.csd_bricked_elems.restype = ctypes.c_longlong
+        lib.csd_to_bricks.argtypes = [ctypes.POINTER(Field), ctypes.c_int, P, P]
+        lib.csd_from_bricks.argtypes = [P, ctypes.c_int, ctypes.POINTER(Field), P]
         lib.csd_grid_size.restype = ctypes.c_size_t
         lib.csd_cfl_update.argtypes = [ctypes.c_int, P, P, ctypes.c_double, ctypes.c_double, P, P]
         lib.csd_grid_build.argtypes = [P, ctypes.POINTER(Field), ctypes.c_int, ctypes.POINTER(Field),
@@ -314,6 +319,81 @@ def cfl_update(smax, scale, cfl: float, dt, dt_max: float = 1e30, stream=None) -
                                    ctypes.c_void_p(stream_handle(stream))))
 
 
+def bricked_shape(shape, brick: int) -> tuple:
+    """Shape of the bricked form of an array: brick-grid extents, then one
+    brick (the reference's to_bricks layout)."""
+    nb = tuple(-(-int(n) // brick) for n in shape)
+    return nb + (brick,) * len(shape)
+
+
+def _bricked_elems(shape, brick: int) -> int:
+    return int(library().csd_bricked_elems((ctypes.c_longlong * len(shape))(*shape), len(shape),
+                                           int(brick)))
+
+
+def to_bricks(flat, brick: int, stream=None):
+    """Device bricked copy of the C-contiguous device array ``flat``."""
+    import torch
+
+    out = torch.empty(bricked_shape(flat.shape, brick), dtype=flat.dtype, device=flat.device)
+    f = field_of(flat)
+    check(library().csd_to_bricks(ctypes.byref(f), int(brick), ctypes.c_void_p(out.data_ptr()),
+                                  ctypes.c_void_p(stream_handle(stream))))
+    return out
+
+
+def from_bricks(bricked, shape, brick: int, out=None, stream=None):
+    """Flat (C-contiguous) array of ``shape`` from its bricked form."""
+    import torch
+
+    shape = tuple(int(n) for n in shape)
+    if bricked.numel() < _bricked_elems(shape, brick):
+        raise ValueError("bricked array is smaller than the bricked form of the shape")
+    if not bricked.is_contiguous():
+        raise ValueError("bricked array must be contiguous")
+    if out is None:
+        out = torch.empty(shape, dtype=bricked.dtype, device=bricked.device)
+    f = field_of(out)
+    check(library().csd_from_bricks(ctypes.c_void_p(bricked.data_ptr()), int(brick),
+                                    ctypes.byref(f), ctypes.c_void_p(stream_handle(stream))))
+    return out
+
+
+def bricked_field(t, shape, brick: int) -> Field:
+    """csd_field of a bricked device array holding a ``shape`` array."""
+    import torch
+
+    shape = tuple(int(n) for n in shape)
+    if not isinstance(t, torch.Tensor) or not t.is_cuda or not t.is_contiguous():
+        raise ValueError("bricked fields must be contiguous CUDA tensors")
+    need = _bricked_elems(shape, brick)
+    if t.numel() < need:
+        raise ValueError(f"bricked field holds {t.numel()} elements, the bricked form of "
+                         f"{shape} needs {need}")
+    f = Field()
+    f.ptr = t.data_ptr()
+    f.ndim = len(shape)
+    f.dtype = 2 if t.dtype == torch.float64 else 1 if t.dtype == torch.float32 else 0
+    if f.dtype == 0:
+        raise TypeError(f"unsupported dtype {t.dtype}")
+    stride = 1
+    for i in reversed(range(len(shape))):
+        f.shape[i] = shape[i]
+        f.strides[i] = stride
+        stride *= shape[i]
+    return f
+
+
+def launch_fields(kernel: NativeKernel, fin, fout, halo, stream=None, **kw) -> None:
+    """csd_launch on prepared csd_field lists."""
+    lib = library()
+    a = (Field * len(fin))(*fin)
+    b = (Field * max(1, len(fout)))(*fout)
+    o = make_opts(halo, **kw)
+    check(lib.csd_launch(kernel.handle, a, len(fin), b, len(fout), ctypes.byref(o),
+                         ctypes.c_void_p(stream_handle(stream))))
+
+
 def error_word(reset: bool = True) -> int:
     v = ctypes.c_int()
     check(library().csd_error_word(ctypes.byref(v), 1 if reset else 0))
@@ -322,5 +402,6 @@ def error_word(reset: bool = True) -> int:
 
 __all__ = ["library", "check", "compile_source", "NativeModule", "NativeKernel", "launch",
            "apply_boundary", "error_word", "CsdError", "field_of", "default_cache_dir",
-           "make_opts", "grid_size", "grid_build", "launch_batch",
+           "make_opts", "grid_size", "grid_build", "launch_batch", "bricked_shape",
+           "to_bricks", "from_bricks", "bricked_field", "launch_fields",
            "CSD_LOADER_TMA", "CSD_LOADER_LDG", "BC_MODES"]

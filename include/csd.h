@@ -174,6 +174,18 @@ int csd_reduce(const csd_field* a, const csd_field* b, const int* halo, int op,
 int csd_reduce_noalloc(const csd_field* a, const csd_field* b, const int* halo, int op,
                        int nblocks, double* result, void* stream);
 
+/* Bricked layout (replaces the generated to_bricks / from_bricks helpers,
+ * multigpu_emitter.py:370-424).  A bricked array stores a 1-3-D array as
+ * bricks of B^ndim elements (B = `brick`, a power of two), bricks row-major
+ * over the brick grid ceil(shape / B), each brick row-major inside; cells of
+ * the padding are zero.  csd_bricked_elems gives the element count of the
+ * bricked buffer.  `flat` must be C-contiguous; both calls are one kernel
+ * launch on `stream`.  A kernel compiled with layout="bricked" reads and
+ * writes fields in this layout (fields described by their flat shape). */
+long long csd_bricked_elems(const long long* shape, int ndim, int brick);
+int csd_to_bricks(const csd_field* flat, int brick, void* bricked, void* stream);
+int csd_from_bricks(const void* bricked, int brick, const csd_field* flat, void* stream);
+
 /* Read (and with reset != 0, clear) the device error word of the current
  * device; synchronises the device. */
 int csd_error_word(int* value, int reset);
