@@ -1084,6 +1084,7 @@ def main() -> None:
     ap.add_argument("--brick", type=int, default=8, help="lap7 bricked: brick size")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--n", type=int, default=512, help="interior extent per dimension")
+    ap.add_argument("--gs-n", type=int, default=4096, help="gray_scott: interior extent")
     ap.add_argument("--serve-requests", type=int, default=2000,
                     help="serve: number of requests in the stream")
     ap.add_argument("--workload", choices=("lap7", "sw_batch", "gray_scott", "serve"),
@@ -1106,8 +1107,9 @@ def main() -> None:
     N_INTERIOR = args.n
     SW_GRIDS, SW_FIXED_N, SW_STEPS = args.sw_grids, args.sw_n, args.sw_steps
     SW_ZCHUNK = args.sw_zchunk
-    global SERVE_REQUESTS
+    global SERVE_REQUESTS, GS_N
     SERVE_REQUESTS = args.serve_requests
+    GS_N = args.gs_n
     if args.warmup < 3:
         args.warmup = 3
     if args.workload == "serve":
