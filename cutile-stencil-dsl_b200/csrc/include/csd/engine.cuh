@@ -307,6 +307,35 @@ struct Loader {
       if constexpr (C::PBUF) {
         if (threadIdx.x < 32) prefetch_wrap(g, ring, bar, slot, x0, y0, z0);
       }
+    } else if constexpr (C::BRICK_SHIFT > 0) {
+      // Bricked fields: every 16-byte group of a box row (X aligned to the
+      // group, bricks at least one group wide) is contiguous in its brick
+      // row, so it moves as one 16-byte copy; groups past the array's X end
+      // are zero-filled in part or whole.
+      constexpr int G = C::ALIGN;
+      constexpr int GW = C::BOXW / G;
+      constexpr int NG = C::ROWS * C::BOXH * GW;
+      static_assert((1 << C::BRICK_SHIFT) >= G, "bricks narrower than a 16-byte group");
+      const long long NZ = g.dims[0], NY = g.dims[1], NX = g.dims[2];
+#pragma unroll 1
+      for (int e = threadIdx.x; e < NG; e += C::NT) {
+        const int xx = (e % GW) * G;
+        const int t = e / GW;
+        const int yy = t % C::BOXH;
+        const int rr = t / C::BOXH;
+        const long long gx = (long long)x0 + xx, gy = (long long)y0 + yy, gz = (long long)z0 + rr;
+        const bool row_ok = gy >= 0 && gy < NY && gz >= 0 && gz < NZ && gx >= 0;
+        long long n = row_ok ? NX - gx : 0;
+        n = n < 0 ? 0 : (n > G ? G : n);
+        const long long off = n > 0 ? elem_off<C>(g, gz, gy, gx) : 0;
+#pragma unroll
+        for (int f = 0; f < C::NIN; ++f) {
+          T* dst = ring + (f * C::NSLOT + slot) * C::SLOT_ELEMS + e * G;
+          const T* src = reinterpret_cast<const T*>(g.in[f]) + off;
+          ptx::cp_async_16_partial(ptx::smem_addr(dst), src, (int)(n * (long long)sizeof(T)));
+        }
+      }
+      ptx::cp_async_arrive(bar);
     } else {
       constexpr int N = C::ROWS * C::BOXH * C::BOXW;
       const long long NZ = g.dims[0], NY = g.dims[1], NX = g.dims[2];

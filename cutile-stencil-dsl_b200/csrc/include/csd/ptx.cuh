@@ -84,6 +84,14 @@ __device__ __forceinline__ void cp_async_zfill(unsigned dst, const void* src, bo
   }
 }
 
+// 16-byte copy global->shared of which the first `src_bytes` (0..16) come
+// from `src` and the rest are zero.
+__device__ __forceinline__ void cp_async_16_partial(unsigned dst, const void* src, int src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src),
+               "r"(src_bytes)
+               : "memory");
+}
+
 // Arrive on `bar` once all of this thread's prior cp.async copies land.
 __device__ __forceinline__ void cp_async_arrive(unsigned bar) {
   asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
