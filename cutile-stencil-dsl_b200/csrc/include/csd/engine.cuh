@@ -260,9 +260,11 @@ struct Loader {
   typedef typename C::T T;
 
   // Warp 0: copy the wrapped (periodic) sources of the chunk's X-halo cells
-  // that an interior point can read into the slot's wrap buffer, then arrive
-  // on the slot barrier once those copies land (32 arrivals per chunk).
-  // Lines outside the interior in Y or Z are left to the synchronous patch.
+  // that an interior point can read into the slot's wrap buffer, each lane
+  // arriving on the slot barrier once its copies land; a chunk away from the
+  // X edges (the decision is the same for the whole warp) has no copies, and
+  // lane 0 makes the 32 arrivals at once.  Lines outside the interior in Y or
+  // Z are left to the synchronous patch.
   static __device__ __forceinline__ void prefetch_wrap(const csd_grid& g, T* ring, unsigned bar,
                                                        int slot, int x0, int y0, int z0) {
     T* pbuf = ring + C::RING_ELEMS + C::INTER_ELEMS + slot * C::PBUF_SLOT;
@@ -288,8 +290,10 @@ struct Loader {
           ptx::cp_async_zfill<sizeof(T)>(ptx::smem_addr(pbuf + u), src, true);
         }
       }
+      ptx::cp_async_arrive(bar);
+    } else if (threadIdx.x == 0) {
+      ptx::mbar_arrive_count(bar, 32u);
     }
-    ptx::cp_async_arrive(bar);
   }
 
   // Issue the copies of one chunk (all fields) of grid `g` into `slot`.

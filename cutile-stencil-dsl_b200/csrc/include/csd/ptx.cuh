@@ -30,6 +30,11 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(unsigned bar, unsigned byt
                : "memory");
 }
 
+// Arrive `count` times at once.
+__device__ __forceinline__ void mbar_arrive_count(unsigned bar, unsigned count) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
   unsigned ok;
   asm volatile(
