@@ -1043,6 +1043,113 @@ def run_serve(args) -> dict | None:
     return line if rank == 0 else None
 
 
+# ---------------------------------------------------------------------------
+# Wide tier: 27- and 125-point boxes at 512^3, eight-in/five-out fused update
+# ---------------------------------------------------------------------------
+WIDE_METRIC = "GPts/s (3-D 125-point box 512^3 sweep, FP64)"
+
+
+def _time_launches(launch, steps: int, warmup: int) -> float:
+    import torch
+
+    for _ in range(warmup):
+        launch()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        launch()
+    e1.record()
+    e1.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def _wide_cpu_job(args):
+    radius, nz, steps = args
+    import numpy as np
+
+    import wide_defs as W
+    from oracle import stencil_oracle as O
+
+    fn = W.load_box(f"cpu_box{radius}", radius, decorated=False)
+    u = np.random.default_rng(1).standard_normal((nz + 2 * radius, 512 + 2 * radius,
+                                                  512 + 2 * radius))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        O.apply_stencil(u, fn, 3, (radius,) * 3)
+    return time.perf_counter() - t0, nz * 512 * 512 * steps
+
+
+def run_wide(args) -> dict | None:
+    import numpy as np
+    import torch
+
+    import wide_defs as W
+    from cutile import compile as stencil_compile
+    from cutile import compile_fused, stencil
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    res = {}
+    with ClockSampler(local) as clk:
+        for radius, name in ((2, "box125"), (1, "box27")):
+            r = stencil_compile(W.load_box(f"{name}_bench", radius), temporal_blocking=False)
+            h = r.halo_widths
+            shape = tuple(512 + 2 * x for x in h)
+            a = torch.zeros(shape, dtype=torch.float64, device="cuda")
+            inner = tuple(slice(x, s - x) for x, s in zip(h, shape))
+            a[inner] = torch.randn((512,) * 3, dtype=torch.float64, device="cuda")
+            b = torch.zeros_like(a)
+            launch = getattr(r.load_module(), f"launch_{r.name}")
+            ms = _time_launches(lambda: launch(a, b), args.steps, args.warmup)
+            res[name] = {"ms": ms, "gpts": 512 ** 3 / ms / 1e6, "tile": list(r.tile_sizes)}
+            del a, b
+        n = 320
+        rc = compile_fused([stencil(ndim=3)(f) for f in W.CNS_MEMBERS], temporal_steps=1)
+        h = rc.halo_widths
+        fields = W.cns_init(n, halo=h)
+        ins = [torch.from_numpy(fields[k]).cuda() for k in rc.inputs]
+        outs = [torch.zeros_like(ins[0]) for _ in W.CNS_MEMBERS]
+        launch = getattr(rc.load_module(), f"launch_{rc.name}")
+        ms = _time_launches(lambda: launch(*ins, *outs), max(3, args.steps // 2), args.warmup)
+        res["cns"] = {"ms": ms, "gpts": n ** 3 / ms / 1e6, "tile": list(rc.tile_sizes)}
+    clocks = clk.summary()
+    peak, peak_kind = _peaks()
+    box = res["box125"]
+    alg = 2 * 8 * 512 ** 3
+    achieved = alg / (box["ms"] / 1e3) / 1e9
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        secs, pts = _wide_cpu_job((2, 8, 1))
+        cpu = {"value": round(pts / secs / 1e9, 6), "unit": "GPts/s", "cores": 1, "kind": "port",
+               "sample": f"1 sweep of an 8x512x512 slab, oracle apply_stencil, {secs:.1f} s"}
+    cns_bytes = (8 + 5) * 8 * n ** 3
+    line = {
+        "metric": WIDE_METRIC, "value": round(box["gpts"], 3), "unit": "GPts/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(box["ms"], 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "dense 5x5x5 box (125 loads, coefficients by distance class, "
+                               "terms grouped by class), 512^3 interior, FP64, halo (2, 2, 16), "
+                               "N(0,1) interior; one sweep per step",
+                   "tile": box["tile"], "parallelism": f"replicas{world}",
+                   "l2": "arrays 1.16 GB >> 126 MB L2"},
+        "comparison": {
+            "box27_gpts": round(res["box27"]["gpts"], 3),
+            "box27_hbm_frac": round(2 * 8 * 512 ** 3 / (res["box27"]["ms"] / 1e3) / 1e9 / peak, 4),
+            "cns_8in_5out_gpts": round(res["cns"]["gpts"], 3),
+            "cns_hbm_frac": round(cns_bytes / (res["cns"]["ms"] / 1e3) / 1e9 / peak, 4),
+            "cns": f"compile_fused of 5 members over 8 fields, {n}^3 FP64, "
+                   f"{cns_bytes / 1e9:.2f} GB algorithmic per launch"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": alg},
+        "e2e": None, "gpu_launches": args.steps, "clocks": clocks, "cpu_baseline": cpu,
+    }
+    return line if rank == 0 else None
+
+
 def run_sw_reference(args) -> dict | None:
     world, rank, _ = _dist()
     if rank != 0:
@@ -1087,7 +1194,7 @@ def main() -> None:
     ap.add_argument("--gs-n", type=int, default=4096, help="gray_scott: interior extent")
     ap.add_argument("--serve-requests", type=int, default=2000,
                     help="serve: number of requests in the stream")
-    ap.add_argument("--workload", choices=("lap7", "sw_batch", "gray_scott", "serve"),
+    ap.add_argument("--workload", choices=("lap7", "sw_batch", "gray_scott", "serve", "wide"),
                     default="lap7",
                     help="lap7: 3-D 7-point 512^3 sweeps; sw_batch: 256 batched shallow-water "
                          "solves; gray_scott: 4096^2 fused Gray-Scott, FP64/FP32/Kahan")
@@ -1112,7 +1219,13 @@ def main() -> None:
     GS_N = args.gs_n
     if args.warmup < 3:
         args.warmup = 3
-    if args.workload == "serve":
+    if args.workload == "wide":
+        if args.impl == "reference":
+            line = {"impl": "reference", "unavailable": "the wide tier is timed against the oracle "
+                    "in its own line's cpu_baseline"}
+        else:
+            line = run_wide(args)
+    elif args.workload == "serve":
         if args.impl == "reference":
             line = {"impl": "reference", "unavailable": "the reference has no serving layer "
                     "(one launch per grid); the plain-path comparison is in the serve line"}
