@@ -922,6 +922,20 @@ def _serve_point_steps(reqs) -> float:
     return tot
 
 
+def _timeline(trace, parts: int = 10):
+    """Iterations and mean active solves in each tenth of the run."""
+    if not trace:
+        return []
+    end = trace[-1][0]
+    out = []
+    for k in range(parts):
+        lo, hi = end * k / parts, end * (k + 1) / parts
+        seg = [t for t in trace if lo <= t[0] < hi or (k == parts - 1 and t[0] == end)]
+        out.append([round(hi, 2), len(seg),
+                    round(sum(t[1] for t in seg) / len(seg), 1) if seg else 0])
+    return out
+
+
 def run_serve(args) -> dict | None:
     import numpy as np
     import torch
@@ -1025,6 +1039,8 @@ def run_serve(args) -> dict | None:
                      f"{alone_mean:.3f} ms); sequential latencies assume FIFO on one GPU",
             "gpts_served": round(gpts, 3),
             "server": {"iterations": st.iterations, "launches": st.launches,
+                       "host_issue_s": round(st.host_s, 3), "gpu_wait_s": round(st.wait_s, 3),
+                       "admit_s": round(st.admit_s, 3), "timeline": _timeline(st.trace),
                        "max_active": st.max_active, "peak_gb": round(st.peak_bytes / 1e9, 3),
                        "rejected": st.rejected, "wall_s": round(st.wall, 3)},
         },

@@ -670,6 +670,7 @@ int csd_launch_batch(csd_kernel* k, const csd_grid* grids, const int* item_start
   memset(&p, 0, sizeof(p));
   p.grids = grids;
   p.item_start = item_start;
+  p.grid_index = opts ? opts->grid_index : nullptr;
   p.ngrids = ngrids;
   p.total_items = total_items;
   p.err = reinterpret_cast<int*>(st->err);

@@ -498,7 +498,7 @@ __device__ __forceinline__ int batch_grid_of(const csd_params& p, int item, int&
     else hi = mid - 1;
   }
   local = item - p.item_start[lo];
-  return lo;
+  return p.grid_index ? p.grid_index[lo] : lo;
 }
 
 // ---------------------------------------------------------------------------

@@ -63,6 +63,7 @@ typedef struct __attribute__((aligned(64))) csd_params {
   csd_grid g;                         // the grid of a single-grid launch
   const csd_grid* grids;              // batched launch: device array (null otherwise)
   const int* item_start;              // batched: prefix sums of items, ngrids + 1 entries
+  const int* grid_index;              // batched: descriptor of batch position k (null = k)
   int ngrids;
   int total_items;
   int* err;                           // device error word (0 = ok)

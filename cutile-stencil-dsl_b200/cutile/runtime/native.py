@@ -53,7 +53,7 @@ class LaunchOpts(ctypes.Structure):
                 ("loader", ctypes.c_int), ("bc_value", ctypes.c_double),
                 ("timeout_ns", ctypes.c_uint64), ("scalars", ctypes.c_double * MAX_SCALARS),
                 ("dyn", ctypes.c_void_p), ("red", ctypes.c_void_p),
-                ("bc_odd", ctypes.c_int * MAX_FIELDS)]
+                ("bc_odd", ctypes.c_int * MAX_FIELDS), ("grid_index", ctypes.c_void_p)]
 
 
 class KernelDesc(ctypes.Structure):
@@ -292,11 +292,12 @@ def grid_build(kernel: NativeKernel, inputs, outputs, halo, dest, **kw) -> tuple
 
 def launch_batch(kernel: NativeKernel, grids_ptr: int, item_start_ptr: int, ngrids: int,
                  total_items: int, stream=None, grid: int = 0, timeout_ns: int = 0,
-                 loader: int = 0) -> None:
+                 loader: int = 0, grid_index_ptr: int | None = None) -> None:
     lib = library()
     o = LaunchOpts()
     o.grid = grid
     o.loader = loader
+    o.grid_index = grid_index_ptr
     o.timeout_ns = timeout_ns
     check(lib.csd_launch_batch(kernel.handle, ctypes.c_void_p(grids_ptr),
                                ctypes.c_void_p(item_start_ptr), ngrids, total_items,

@@ -86,6 +86,7 @@ class _Active:
     phase: int = 0
     done: int = 0
     nbytes: int = 0
+    slot: int = -1             # first of its `phases` descriptor slots in the device pool
 
 
 @dataclass
@@ -97,6 +98,9 @@ class ServerStats:
     admitted: int = 0
     rejected: int = 0
     wall: float = 0.0
+    host_s: float = 0.0        # building and issuing iterations
+    admit_s: float = 0.0       # admitting solves (allocation, initial fields, descriptors)
+    wait_s: float = 0.0        # waiting for the GPU to finish iterations
     trace: list = field(default_factory=list)   # (time, active, used_bytes) per iteration
 
 
@@ -129,7 +133,15 @@ class StencilServer:
             device = torch.device("cuda", torch.cuda.current_device())
         self.device = torch.device(device)
         self._progs: dict = {}
-        self._dev_desc: dict = {}
+        self._idx_bufs: dict = {}
+        self._pool = None          # device descriptors of every active solve, all phases
+        self._pool_top = 0
+        self._pool_free: dict = {}  # phases -> free slot blocks
+        self._gen = None
+        self._reserved = False
+        # host time admissions may take before the next iteration is issued,
+        # so that a burst of arrivals does not leave the GPU idle
+        self.admit_budget_s = 0.002
         self.stats = ServerStats()
 
     # -- programs ----------------------------------------------------------
@@ -183,10 +195,11 @@ class StencilServer:
                 t = a if isinstance(a, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(a))
                 bufs[(-k) % P].copy_(t.to(device=self.device, dtype=tdt), non_blocking=True)
         else:
-            g = torch.Generator(device=self.device)
-            g.manual_seed(int(req.seed))
+            if self._gen is None:
+                self._gen = torch.Generator(device=self.device)
+            self._gen.manual_seed(int(req.seed))
             interior = tuple(s - 2 * h for h, s in zip(halo, req.shape))
-            u = torch.rand(interior, generator=g, device=self.device, dtype=tdt)
+            u = torch.rand(interior, generator=self._gen, device=self.device, dtype=tdt)
             for k in range(kind.nstate):
                 bufs[(-k) % P][inner].copy_(u)
         gsz = native.grid_size()
@@ -198,36 +211,68 @@ class StencilServer:
             items, loader = native.grid_build(kern, ins, out, halo, desc[p].ctypes.data,
                                               zchunk=zc, loader=native.CSD_LOADER_TMA)
         res.admitted = now
+        slot = self._pool_alloc(P)
+        gsz = native.grid_size()
+        self._pool[slot * gsz:(slot + P) * gsz].copy_(
+            torch.from_numpy(desc.reshape(-1)).pin_memory(), non_blocking=True)
         return _Active(req=req, res=res, flat=flat, bufs=bufs, desc=desc, items=items,
-                       nbytes=flat.numel() * flat.element_size())
+                       nbytes=flat.numel() * flat.element_size(), slot=slot)
+
+    # -- the device descriptor pool ---------------------------------------
+    def _pool_alloc(self, n: int) -> int:
+        """First slot of `n` consecutive descriptor slots.  Growing copies the
+        pool on the stream, after the launches that read the old one."""
+        import torch
+
+        free = self._pool_free.get(n)
+        if free:
+            return free.pop()
+        gsz = native.grid_size()
+        cap = 0 if self._pool is None else self._pool.numel() // gsz
+        if self._pool_top + n > cap:
+            new_cap = max(256, 2 * cap, self._pool_top + n)
+            pool = torch.empty(new_cap * gsz, dtype=torch.uint8, device=self.device)
+            if self._pool is not None:
+                pool[:self._pool_top * gsz].copy_(self._pool[:self._pool_top * gsz])
+            self._pool = pool
+        slot = self._pool_top
+        self._pool_top += n
+        return slot
+
+    def _pool_release(self, slot: int, n: int) -> None:
+        self._pool_free.setdefault(n, []).append(slot)
 
     # -- one iteration -----------------------------------------------------
     def _iterate(self, active: list, stream) -> None:
+        """Issue one step of every active solve: per (kind, dtype) group, the
+        batch's descriptor indices (pool slot + phase) and item prefix sums go
+        up in one pinned copy and one batched launch reads the resident
+        descriptors.  Index buffers alternate between iterations; the loop
+        keeps at most two iterations in flight, so a buffer is rewritten only
+        after the launch that read it has finished."""
         import numpy as np
         import torch
 
         groups: dict = {}
         for a in active:
             groups.setdefault((a.req.kind, a.req.dtype), []).append(a)
-        gsz = native.grid_size()
+        parity = self.stats.iterations & 1
         for key, members in groups.items():
             prog, kern, zc = self.program(*key)
             n = len(members)
-            host = np.concatenate([a.desc[a.phase] for a in members])
-            starts = np.zeros(n + 1, dtype=np.int32)
-            np.cumsum([a.items for a in members], out=starts[1:])
-            buf = self._dev_desc.get(key)
-            if buf is None or buf[0].numel() < host.size or buf[1].numel() < n + 1:
-                cap = max(host.size, 64 * gsz) * 2
-                buf = (torch.empty(cap, dtype=torch.uint8, device=self.device),
-                       torch.empty(2 * (n + 1) + 64, dtype=torch.int32, device=self.device))
-                self._dev_desc[key] = buf
-            # the previous iteration's launch has finished (host sync), so the
-            # device work list can be overwritten
-            buf[0][:host.size].copy_(torch.from_numpy(host), non_blocking=False)
-            buf[1][:n + 1].copy_(torch.from_numpy(starts), non_blocking=False)
-            native.launch_batch(kern, buf[0].data_ptr(), buf[1].data_ptr(), n, int(starts[-1]),
-                                stream, loader=native.CSD_LOADER_TMA)
+            host = np.empty(2 * n + 1, dtype=np.int32)
+            host[:n] = [a.slot + a.phase for a in members]
+            host[n] = 0
+            np.cumsum([a.items for a in members], out=host[n + 1:])
+            bufs = self._idx_bufs.setdefault(key, [None, None])
+            buf = bufs[parity]
+            if buf is None or buf.numel() < host.size:
+                buf = torch.empty(max(2 * host.size, 1024), dtype=torch.int32, device=self.device)
+                bufs[parity] = buf
+            buf[:host.size].copy_(torch.from_numpy(host).pin_memory(), non_blocking=True)
+            native.launch_batch(kern, self._pool.data_ptr(), buf.data_ptr() + 4 * n, n,
+                                int(host[-1]), stream, loader=native.CSD_LOADER_TMA,
+                                grid_index_ptr=buf.data_ptr())
             self.stats.launches += 1
 
     def _stream(self):
@@ -235,8 +280,35 @@ class StencilServer:
 
         return torch.cuda.current_stream(self.device)
 
-    def _sync(self, stream) -> None:
-        stream.synchronize()
+    def _reserve(self) -> None:
+        """Have the caching allocator hold the budget's memory as one free
+        segment before serving: admissions then split it instead of calling
+        cudaMalloc (which synchronises the device) in the request loop."""
+        import torch
+
+        if self._reserved:
+            return
+        self._reserved = True
+        free, _total = torch.cuda.mem_get_info(self.device)
+        nbytes = int(min(self.budget, 0.9 * free))
+        if nbytes > 0:
+            block = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+            del block
+
+    def _record(self, stream):
+        """A marker after the work issued so far on ``stream``."""
+        import torch
+
+        ev = torch.cuda.Event(enable_timing=True)
+        ev.record(stream)
+        return ev
+
+    def _wait(self, mark) -> None:
+        mark.synchronize()
+
+    def _mark_time(self, mark, start, t_start: float) -> float:
+        """Seconds after the loop start at which the GPU passed ``mark``."""
+        return t_start + start.elapsed_time(mark) / 1e3
 
     # -- the request loop --------------------------------------------------
     def run(self, requests, *, realtime: bool = True, keep_state=True):
@@ -245,7 +317,9 @@ class StencilServer:
         admissible only once the wall clock passes its arrival time.
         ``keep_state``: True, False or a set of request ids whose final
         fields the results keep (kept fields stay allocated after the budget
-        has released them)."""
+        has released them).  The host builds and issues iteration k + 1 while
+        the GPU runs iteration k; a solve's completion time is when the GPU
+        passed the end of its last iteration."""
         reqs = list(requests)
         for i, r in enumerate(reqs):
             if r.rid < 0:
@@ -254,14 +328,22 @@ class StencilServer:
                                       steps=r.steps, arrival=r.arrival) for r in reqs}
         queue = deque(sorted(reqs, key=lambda r: (r.arrival, r.rid)))
         active: list[_Active] = []
+        in_flight: deque = deque()          # (marker, solves finished by it)
         used = 0
         stream = self._stream()
+        self._reserve()
+        start = self._record(stream)
+        self._wait(start)           # the GPU clock's zero is the loop start
         t0 = time.perf_counter()
         st = self.stats
-        while queue or active:
+        while queue or active or in_flight:
             now = time.perf_counter() - t0
-            # admit arrived requests in order while they fit
+            # admit arrived requests in order while they fit (a bounded amount
+            # of host time per pass while solves are running)
+            admit_until = time.perf_counter() + self.admit_budget_s
             while queue and (not realtime or queue[0].arrival <= now):
+                if (active or in_flight) and time.perf_counter() > admit_until:
+                    break
                 r = queue[0]
                 need = self.memory_of(r)
                 if need > self.budget:
@@ -273,36 +355,53 @@ class StencilServer:
                 if used + need > self.budget:
                     break                       # first come, first served
                 queue.popleft()
+                ta = time.perf_counter()
                 a = self._admit(r, results[r.rid], now)
+                st.admit_s += time.perf_counter() - ta
                 active.append(a)
                 used += a.nbytes
                 st.admitted += 1
             st.peak_bytes = max(st.peak_bytes, used)
             st.max_active = max(st.max_active, len(active))
-            if not active:
-                if queue and realtime:
-                    time.sleep(max(0.0, min(queue[0].arrival - now, 0.01)))
-                continue
-            self._iterate(active, stream)
-            self._sync(stream)
-            now = time.perf_counter() - t0
-            st.iterations += 1
-            st.trace.append((now, len(active), used))
-            keep = []
-            for a in active:
-                a.done += 1
-                a.phase = (a.phase + 1) % len(a.bufs)
-                if a.done >= a.req.steps:
-                    res = a.res
-                    res.completed = now
-                    P = len(a.bufs)
-                    nstate = self.kinds[a.req.kind].nstate
-                    if keep_state is True or (keep_state and a.req.rid in keep_state):
-                        res.state = tuple(a.bufs[(a.phase - k) % P] for k in range(nstate))
-                    used -= a.nbytes
-                else:
-                    keep.append(a)
-            active = keep
+            if active:
+                th = time.perf_counter()
+                self._iterate(active, stream)
+                mark = self._record(stream)
+                st.host_s += time.perf_counter() - th
+                st.iterations += 1
+                st.trace.append((time.perf_counter() - t0, len(active), used))
+                finished, keep = [], []
+                for a in active:
+                    a.done += 1
+                    a.phase = (a.phase + 1) % len(a.bufs)
+                    if a.done >= a.req.steps:
+                        P = len(a.bufs)
+                        nstate = self.kinds[a.req.kind].nstate
+                        if keep_state is True or (keep_state and a.req.rid in keep_state):
+                            a.res.state = tuple(a.bufs[(a.phase - k) % P] for k in range(nstate))
+                        # later work on the stream is ordered after this
+                        # iteration, so the memory and slots can be reused now
+                        used -= a.nbytes
+                        if a.slot >= 0:
+                            self._pool_release(a.slot, P)
+                        finished.append(a.res)
+                    else:
+                        keep.append(a)
+                active = keep
+                in_flight.append((mark, finished))
+            # keep one iteration in flight while the next is prepared
+            while in_flight and (len(in_flight) > 1 or not active):
+                mark, finished = in_flight.popleft()
+                tw = time.perf_counter()
+                self._wait(mark)
+                st.wait_s += time.perf_counter() - tw
+                if finished:
+                    tdone = self._mark_time(mark, start, 0.0)
+                    for res in finished:
+                        res.completed = tdone
+            if not active and not in_flight and queue and realtime:
+                now = time.perf_counter() - t0
+                time.sleep(max(0.0, min(queue[0].arrival - now, 0.01)))
         st.wall = time.perf_counter() - t0
         return [results[r.rid] for r in reqs]
 

@@ -62,6 +62,9 @@ typedef struct csd_launch_opts {
   const double* dyn;    /* device array of per-grid dynamic scalars (e.g. dt), or NULL */
   double* red;          /* device double receiving a max-reduction, or NULL */
   int bc_odd[CSD_MAX_FIELDS];       /* per field: bit d = sign flip when mirrored in dim d */
+  const int* grid_index;  /* csd_launch_batch: device map from batch position to descriptor
+                             index in `grids` (NULL = identity), so descriptors can stay
+                             resident in a pool while the batch changes */
 } csd_launch_opts;
 
 /* Library version (major*100 + minor). */

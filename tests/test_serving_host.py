@@ -29,8 +29,19 @@ class FakeServer(StencilServer):
     def _stream(self):
         return None
 
-    def _sync(self, stream):
+    def _reserve(self):
         pass
+
+    def _record(self, stream):
+        import time
+
+        return time.perf_counter()
+
+    def _wait(self, mark):
+        pass
+
+    def _mark_time(self, mark, start, t_start):
+        return t_start + (mark - start)
 
 
 KINDS = [SolveKind("heat2d", {}, 1), SolveKind("wave2d", {}, 2), SolveKind("lap7", {}, 1)]
