@@ -52,6 +52,19 @@ def _peaks():
     return 6650.0, "fallback"
 
 
+def _max_over_ranks(value: float) -> float:
+    """The largest ``value`` over all ranks (the process group's backend
+    decides the device: CUDA for NCCL, host for gloo)."""
+    import torch
+
+    if not torch.distributed.is_initialized() or torch.distributed.get_world_size() == 1:
+        return float(value)
+    dev = "cuda" if torch.distributed.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 def _dist():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -193,9 +206,7 @@ def run_ours(args) -> dict:
         barrier()
     ms = ev0.elapsed_time(ev1)
     if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = _max_over_ranks(ms)
     clocks = clk.summary()
     ms_per_step = ms / args.steps
     gpts = npts * T * args.steps / (ms / 1e3) / 1e9 * world
@@ -232,9 +243,7 @@ def run_ours(args) -> dict:
     e2e_wall = (time.perf_counter() - t0) * 1e3 / e2e_steps
     e2e_ms = max(e2e_ms, e2e_wall)
     if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+        e2e_ms = _max_over_ranks(e2e_ms)
     e2e_gpts = npts * T * sweeps / (e2e_ms / 1e3) / 1e9 * world
 
     traffic = _profiled_traffic(args.dtype, T)
@@ -483,9 +492,7 @@ def run_sw_batch(args) -> dict | None:
         barrier()
         ms = ev0.elapsed_time(ev1)
         if world > 1:
-            t = torch.tensor([ms], device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms = float(t.item())
+            ms = _max_over_ranks(ms)
         return ms / steps
 
     runs = {}
@@ -753,9 +760,7 @@ def run_gray_scott(args) -> dict | None:
             clocks = clk.summary()
         ms = ev0.elapsed_time(ev1)
         if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms = float(t.item())
+            ms = _max_over_ranks(ms)
         inner = tuple(slice(x, sz - x) for x, sz in zip(h, u0.shape))
         runs[prec] = {"ms": ms, "u": a[0][inner].double(), "v": a[1][inner].double(),
                       "itemsize": np.dtype(dtype).itemsize, "h": h, "step": step,
@@ -972,9 +977,7 @@ def run_serve(args) -> dict | None:
     span = max(r.completed for r in done) - min(r.arrival for r in reqs)
     solves_s = len(done) / span
     if world > 1:
-        t = torch.tensor([span], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        solves_s = len(done) * world / float(t.item())
+        solves_s = len(done) * world / _max_over_ranks(span)
     gpts = _serve_point_steps([r for r in reqs]) / span / 1e9
 
     # each request alone on the plain path (drop-in launch per step), sampled
