@@ -595,6 +595,23 @@ static int build_grid(csd_kernel* k, const csd_field* in, int n_in, const csd_fi
                                             2 /*L2 promotion 128B*/, 0 /*OOB fill zeros*/);
       if (r) return cu_fail(r, "cuTensorMapEncodeTiled");
     }
+    const int rx1 = D.temporal > 0 ? D.rx / D.temporal : D.rx;
+    if (D.bc_mode == CSD_BC_PERIODIC && rx1 > 0) {
+      // narrow boxes for the periodic X wrap (engine.cuh: Cfg::WRAPW)
+      const unsigned wrapw = (unsigned)(((rx1 + D.align - 1) / D.align) * D.align + D.align);
+      for (int i = 0; i < n_in; ++i) {
+        unsigned long long gdim[3] = {(unsigned long long)g->dims[2], (unsigned long long)g->dims[1],
+                                      (unsigned long long)g->dims[0]};
+        unsigned long long gstride[2] = {(unsigned long long)(g->pitch_y * esz),
+                                         (unsigned long long)(g->pitch_z * esz)};
+        unsigned box[3] = {wrapw, (unsigned)D.box_h, (unsigned)D.rows};
+        unsigned estride[3] = {1, 1, 1};
+        CUresult r = d.cuTensorMapEncodeTiled(&g->tmap_wrap[i],
+                                              esz == 8 ? TMAP_FLOAT64 : TMAP_FLOAT32, 3, in[i].ptr,
+                                              gdim, gstride, box, estride, 0, 0, 2, 0);
+        if (r) return cu_fail(r, "cuTensorMapEncodeTiled(wrap)");
+      }
+    }
   }
   *loader_out = loader;
   return CSD_OK;

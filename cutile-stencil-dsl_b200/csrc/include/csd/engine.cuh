@@ -87,12 +87,16 @@ struct Cfg {
   }
   static constexpr int RING_ELEMS = NIN * NSLOT * SLOT_ELEMS;
   static constexpr int INTER_ELEMS = inter_elems_upto(TEMPORAL);
-  // Periodic X wrap (TMA loader): the wrapped source cells of a chunk's X
-  // halo lines are copied ahead with cp.async into a per-slot buffer,
-  // indexed ((field * PLINES + line) * 2 + side) * RX + layer.
+  // Periodic X wrap (TMA loader): for a chunk at an X edge, a narrow TMA box
+  // of WRAPW columns from the far side of the same rows lands with the chunk
+  // in a per-slot wrap buffer: per field, a left and a right block of
+  // ROWS x BOXH x WRAPW, each block 128-byte aligned.
   static constexpr int PLINES = ROWS * BOXH;
   static constexpr int PBUF = (BC == CSD_BC_PERIODIC && LOADER == CSD_LOADER_TMA && RX > 0) ? 1 : 0;
-  static constexpr int PBUF_SLOT = PBUF ? align_up(NIN * PLINES * 2 * RX, 16) : 0;
+  static constexpr int WRAPW = align_up(RX, ALIGN) + ALIGN;
+  static constexpr int WRAP_ELEMS = ROWS * BOXH * WRAPW;
+  static constexpr int WRAP_BLOCK = align_up(WRAP_ELEMS, 128 / (int)sizeof(T));
+  static constexpr int PBUF_SLOT = PBUF ? NIN * 2 * WRAP_BLOCK : 0;
   static constexpr int PBUF_ELEMS = NSLOT * PBUF_SLOT;
   static constexpr int BAR_OFFSET = (RING_ELEMS + INTER_ELEMS + PBUF_ELEMS) * (int)sizeof(T);
   // +128: the dynamic shared-memory base is aligned up to 128 bytes in the kernel
@@ -259,41 +263,14 @@ template <class C>
 struct Loader {
   typedef typename C::T T;
 
-  // Warp 0: copy the wrapped (periodic) sources of the chunk's X-halo cells
-  // that an interior point can read into the slot's wrap buffer, each lane
-  // arriving on the slot barrier once its copies land; a chunk away from the
-  // X edges (the decision is the same for the whole warp) has no copies, and
-  // lane 0 makes the 32 arrivals at once.  Lines outside the interior in Y or
-  // Z are left to the synchronous patch.
-  static __device__ __forceinline__ void prefetch_wrap(const csd_grid& g, T* ring, unsigned bar,
-                                                       int slot, int x0, int y0, int z0) {
-    T* pbuf = ring + C::RING_ELEMS + C::INTER_ELEMS + slot * C::PBUF_SLOT;
-    const int hz = g.halo[0], hy = g.halo[1], hx = g.halo[2];
-    const int nz = g.interior[0], ny = g.interior[1], nx = g.interior[2];
-    const bool touches = x0 < hx || x0 + C::BOXW > hx + nx;
-    if (touches) {
-      constexpr int UNITS = C::NIN * C::PLINES * 2 * C::RX;
-      for (int u = threadIdx.x; u < UNITS; u += 32) {
-        const int k = u % C::RX;
-        const int side = (u / C::RX) & 1;
-        const int line = (u / (2 * C::RX)) % C::PLINES;
-        const int f = u / (2 * C::RX * C::PLINES);
-        const int yy = line % C::BOXH;
-        const int rr = line / C::BOXH;
-        const long long gy = (long long)y0 + yy, gz = (long long)z0 + rr;
-        const long long gx = side ? (long long)hx + nx + k : (long long)hx - C::RX + k;
-        const bool ok = gx >= x0 && gx < (long long)x0 + C::BOXW && gx >= 0 && gx < g.dims[2] &&
-                        (gy >= hy && gy < hy + ny) && (gz >= hz && gz < hz + nz);
-        if (ok) {
-          const long long mx = bc_map(gx, hx, nx, CSD_BC_PERIODIC);
-          const T* src = reinterpret_cast<const T*>(g.in[f]) + gz * g.pitch_z + gy * g.pitch_y + mx;
-          ptx::cp_async_zfill<sizeof(T)>(ptx::smem_addr(pbuf + u), src, true);
-        }
-      }
-      ptx::cp_async_arrive(bar);
-    } else if (threadIdx.x == 0) {
-      ptx::mbar_arrive_count(bar, 32u);
-    }
+  // X origins of the wrap boxes of a periodic chunk at (x0): the left halo
+  // cells [hx - RX, hx) take columns [hx - RX + nx, hx + nx), the right halo
+  // cells [hx + nx, hx + nx + RX) take [hx, hx + RX); each box starts at the
+  // 16-byte boundary at or below its first column.
+  static __device__ __forceinline__ int wrap_x(const csd_grid& g, int side) {
+    const int hx = g.halo[2], nx = g.interior[2];
+    const int first = side ? hx : hx - C::RX + nx;
+    return (first / C::ALIGN) * C::ALIGN;
   }
 
   // Issue the copies of one chunk (all fields) of grid `g` into `slot`.
@@ -301,15 +278,31 @@ struct Loader {
                                                int x0, int y0, int z0) {
     if constexpr (C::LOADER == CSD_LOADER_TMA) {
       if (threadIdx.x == 0) {
-        ptx::mbar_arrive_expect_tx(bar, (unsigned)(C::CHUNK_BYTES * C::NIN));
+        bool left = false, right = false;
+        if constexpr (C::PBUF) {
+          left = x0 < g.halo[2];
+          right = x0 + C::BOXW > g.halo[2] + g.interior[2];
+        }
+        const unsigned wrap_bytes = (unsigned)(C::WRAP_ELEMS * sizeof(T) * C::NIN);
+        ptx::mbar_arrive_expect_tx(bar, (unsigned)(C::CHUNK_BYTES * C::NIN) +
+                                            (left ? wrap_bytes : 0u) + (right ? wrap_bytes : 0u));
 #pragma unroll
         for (int f = 0; f < C::NIN; ++f) {
           T* dst = ring + (f * C::NSLOT + slot) * C::SLOT_ELEMS;
           ptx::tma_load_3d(ptx::smem_addr(dst), &g.tmap[f], x0, y0, z0, bar);
         }
-      }
-      if constexpr (C::PBUF) {
-        if (threadIdx.x < 32) prefetch_wrap(g, ring, bar, slot, x0, y0, z0);
+        if constexpr (C::PBUF) {
+          T* pbuf = ring + C::RING_ELEMS + C::INTER_ELEMS + slot * C::PBUF_SLOT;
+#pragma unroll
+          for (int f = 0; f < C::NIN; ++f) {
+            if (left)
+              ptx::tma_load_3d(ptx::smem_addr(pbuf + (f * 2 + 0) * C::WRAP_BLOCK),
+                               &g.tmap_wrap[f], wrap_x(g, 0), y0, z0, bar);
+            if (right)
+              ptx::tma_load_3d(ptx::smem_addr(pbuf + (f * 2 + 1) * C::WRAP_BLOCK),
+                               &g.tmap_wrap[f], wrap_x(g, 1), y0, z0, bar);
+          }
+        }
       }
     } else if constexpr (C::BRICK_SHIFT > 0) {
       // Bricked fields: every 16-byte group of a box row (X aligned to the
@@ -421,14 +414,16 @@ __device__ __forceinline__ void patch_x_cell(const csd_grid& g, typename C::T* r
     return;
   }
   const T* pbuf = ring + C::RING_ELEMS + C::INTER_ELEMS + slot * C::PBUF_SLOT;
-  const int k = side ? (int)(gx - hx - nx) : (int)(gx - (hx - C::RX));
-  const int sx = (int)(bc_map(gx, hx, nx, C::BC) - x0);  // source box column (same line)
+  const long long src = bc_map(gx, hx, nx, C::BC);
+  const int sx = (int)(src - x0);  // source box column (same line)
+  // periodic: column of the source in its wrap block
+  const int wx = C::PBUF ? (int)(src - Loader<C>::wrap_x(g, side)) : 0;
 #pragma unroll
   for (int f = 0; f < C::NIN; ++f) {
     T* slot_base = ring + (f * C::NSLOT + slot) * C::SLOT_ELEMS;
     T v;
     if (C::BC == CSD_BC_PERIODIC) {
-      v = pbuf[((f * C::PLINES + line) * 2 + side) * C::RX + k];
+      v = pbuf[(f * 2 + side) * C::WRAP_BLOCK + line * C::WRAPW + wx];
     } else {
       v = slot_base[line * C::BOXW + sx];
       if (C::BC == CSD_BC_REFLECTING && odd_flip<C>(g, f, true, false, false)) v = -v;
@@ -528,7 +523,7 @@ __device__ __forceinline__ void stream_engine(const csd_params& p) {
 #pragma unroll 1
     for (int s = 0; s < C::NSLOT; ++s)
       ptx::mbar_init(ptx::smem_addr(&bars[s]),
-                     C::LOADER == CSD_LOADER_TMA ? 1u + (C::PBUF ? 32u : 0u) : (unsigned)C::NT);
+                     C::LOADER == CSD_LOADER_TMA ? 1u : (unsigned)C::NT);
     ptx::fence_mbar_init();
   }
   // Zero the intermediate rings once: rows/columns a stage never writes are

@@ -56,6 +56,9 @@ typedef struct __attribute__((aligned(64))) csd_grid {
   // brick row-major inside; nbx / nby bricks along X / Y of the padded array.
   int brick_shift;                    // 0: flat (pitched) layout
   int nbx, nby;
+  // Periodic-X kernels (TMA loader): narrow boxes (wrap width x box height x
+  // rows) of the inputs, loaded from the far side of a row for X-edge chunks.
+  csd_tmap tmap_wrap[CSD_MAX_FIELDS];
 } csd_grid;
 
 // Kernel parameter: one grid inline, or a device array of grids.

@@ -204,7 +204,8 @@ def engine_geometry(plan: EnginePlan, radius3: tuple[int, int, int], dtype_bytes
     slot_elems = _align_up(plan.rows * box_h * box_w, per128)
     inter = sum(nslot_i * _align_up(plan.rows * (plan.tile_y + 2 * (T - s) * ry) * box_w, per128)
                 for s in range(1, T))
-    pbuf_slot = _align_up(num_inputs * plan.rows * box_h * 2 * rx, 16) if rx > 0 else 0
+    wrapw = _align_up(rx, align) + align
+    pbuf_slot = num_inputs * 2 * _align_up(plan.rows * box_h * wrapw, per128) if rx > 0 else 0
     smem = ((num_inputs * nslot * slot_elems + inter + nslot * pbuf_slot) * dtype_bytes
             + 8 * nslot + 64 + 128)
     return {"align": align, "pad_left": pad_left, "box_w": box_w, "box_h": box_h,
