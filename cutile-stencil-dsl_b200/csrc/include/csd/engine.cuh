@@ -184,6 +184,10 @@ __device__ __forceinline__ void store_vec(float* p, const float* v) {
 __device__ __forceinline__ long long bc_map(long long i, int h, int n, int mode) {
   if (i >= h && i < h + n) return i;
   if (mode == CSD_BC_PERIODIC) {
+    // one wrap covers every cell within a radius <= n of the interior; the
+    // 64-bit remainder (a long software sequence) is only for wider halos
+    if (i < h && i + n >= h) return i + n;
+    if (i >= h + n && i - n < h + n) return i - n;
     long long k = (i - h) % n;
     if (k < 0) k += n;
     return h + k;
@@ -473,8 +477,9 @@ __device__ __forceinline__ void patch_boundary(const csd_grid& g, typename C::T*
         patch_x_cell<C>(g, ring, slot, line, xx, x0, gy, gz, 1);
     }
   }
-  // the slot will be refilled by TMA (async proxy) after these generic writes
-  ptx::fence_proxy_async_smem();
+  // The slot is refilled by TMA (async proxy) only after a block barrier and
+  // the issuing thread's proxy fence (the refill path), which orders these
+  // generic writes before it.
 }
 
 __device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
