@@ -25,13 +25,13 @@ zeroed, so a zero Dirichlet halo stays zero (kernels write interiors only).
 
 from __future__ import annotations
 
-import ctypes
 import math
 import time
 from collections import deque
 from dataclasses import dataclass, field
 
 from cutile.runtime import native
+from cutile.runtime.rk_runtime import batch_zchunk
 
 
 @dataclass
@@ -111,14 +111,6 @@ def percentile(values, q: float) -> float:
         return math.nan
     k = max(0, min(len(v) - 1, math.ceil(q / 100.0 * len(v)) - 1))
     return v[k]
-
-
-def batch_zchunk(kernel: native.NativeKernel) -> int:
-    """Rows per work item in a batched launch: short items for issue-bound
-    bodies (kernels whose default asks for several items per resident
-    block), long ones for memory-bound bodies."""
-    d = kernel.desc
-    return 2 * d["rows"] if d["zchunk"] < 0 else 64
 
 
 class StencilServer:

@@ -165,3 +165,34 @@ def test_sw_batch_row_pitched_equals_contiguous():
     for a, b in zip(st_c, st_p):
         for x, y in zip(a, b):
             assert torch.equal(x, y)
+
+
+@pytest.mark.parametrize("method", ["rk4", "ssprk3"])
+def test_batch_of_other_methods_equals_single_grid_steps(method):
+    """Batched stages of RK4 / SSPRK3 (accumulator and convex-combination
+    forms) give each grid the bits of its own single-grid steps."""
+    import torch
+
+    from cutile import RKIntegrator
+    from cutile.runtime.rk_runtime import RKBatch
+
+    rk = RKIntegrator(_stencil(heat_op, 2), method).compile()
+    h = rk.info["halo"]
+    rng = np.random.default_rng(9)
+    shapes = [(30, 41), (57, 33), (64, 64)]
+    grids = []
+    for n0, n1 in shapes:
+        u = np.zeros((n0 + 2 * h[0], n1 + 2 * h[1]))
+        u[h[0]:-h[0], h[1]:-h[1]] = rng.random((n0, n1))
+        grids.append(u)
+    batched = [(torch.from_numpy(u).cuda(),) for u in grids]
+    b = RKBatch(rk, batched, dt=0.05)
+    single = [torch.from_numpy(u).cuda() for u in grids]
+    step = getattr(rk.load_module(), f"rk_{method}_step")
+    for _ in range(4):
+        b.step()
+        for t in single:
+            step(t, 0.05)
+    torch.cuda.synchronize()
+    for (x,), y in zip(batched, single):
+        assert torch.equal(x, y)

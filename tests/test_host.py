@@ -253,3 +253,68 @@ def test_pack_grids_rows_are_aligned_for_tma():
     ends = sorted((t.storage_offset(), t.storage_offset() + t.stride(0) * t.shape[0])
                   for g in grids for t in g)
     assert all(a[1] <= b[0] for a, b in zip(ends, ends[1:]))
+
+
+def test_autotune_candidates_fit_and_are_distinct():
+    from cutile.passes.tiling import B200_SMEM_PER_BLOCK, engine_geometry, radius3
+    from cutile.runtime.autotune import cache_key, candidates
+
+    for ndim, db, radius, nin, single in ((3, 8, (1, 1, 1), 1, True), (3, 4, (2, 2, 2), 1, True),
+                                          (2, 8, (1, 1), 3, False), (1, 4, (4,), 1, True)):
+        plans = candidates(ndim, db, radius, nin, 7, 20, single)
+        assert 1 < len(plans) <= 30
+        keys = {(p.rows, p.tile_y, p.tile_x, p.threads, p.stages, p.temporal, p.min_blocks)
+                for p in plans}
+        assert len(keys) == len(plans)
+        for p in plans:
+            g = engine_geometry(p, radius3(ndim, radius), db, nin)
+            assert g["smem_bytes"] <= B200_SMEM_PER_BLOCK and g["box_w"] <= 256
+            assert single or p.temporal == 1
+    fp = {"radius": [1, 1, 1], "loads": 7, "inputs": 1, "outputs": 1, "body_ops": 20}
+    assert cache_key(fp, "float64", (512,) * 3, "B200") == cache_key(fp, "float64", (512,) * 3, "B200")
+    assert cache_key(fp, "float64", (512,) * 3, "B200") != cache_key(fp, "float32", (512,) * 3, "B200")
+    assert cache_key(fp, "float64", (512,) * 3, "B200") != cache_key(fp, "float64", (128,) * 3, "B200")
+
+
+def test_regcheck_selection_rules():
+    from cutile.runtime.regcheck import (Config, Resources, parse_ptxas_log, register_budget,
+                                         select_config, select_fastest)
+
+    assert register_budget(occupancy=4) == 128 and register_budget(2) == 256
+    cfgs = [Config((1, 4, 128), {"k": 0}), Config((1, 8, 64), {"k": 1}), Config((1, 2, 32), {"k": 2})]
+    res = {0: Resources(200, 0), 1: Resources(90, 0), 2: Resources(60, 0)}
+    assert select_config(cfgs, lambda c: res[c.kernel_hints["k"]], max_registers=128) is cfgs[1]
+    spill = {0: Resources(128, 64, spill_bytes=64), 1: Resources(128, 32, spill_bytes=32),
+             2: Resources(255, 8, spill_bytes=8)}
+    assert select_config(cfgs, lambda c: spill[c.kernel_hints["k"]]) is cfgs[2]
+    timed = {0: Resources(64, 0, ms=1.00), 1: Resources(64, 0, ms=0.99), 2: Resources(64, 0, ms=0.5)}
+    assert select_fastest(cfgs, lambda c: timed[c.kernel_hints["k"]]) is cfgs[2]
+    near = {0: Resources(64, 0, ms=1.02), 1: Resources(64, 0, ms=1.0), 2: Resources(64, 0, ms=1.5)}
+    assert select_fastest(cfgs, lambda c: near[c.kernel_hints["k"]]) is cfgs[0]   # within 3 %
+    log = ("ptxas info    : Compiling entry function 'k_tma' for 'sm_100a'\n"
+           "ptxas info    : Function properties for k_tma\n"
+           "ptxas         .     8 bytes stack frame, 4 bytes spill stores, 4 bytes spill loads\n"
+           "ptxas info    : Used 96 registers, used 1 barriers, 128 bytes smem\n")
+    r = parse_ptxas_log(log, "k_tma")
+    assert r.registers == 96 and r.stack_bytes == 8 and r.spill_bytes == 4 and r.spills
+
+
+def test_serving_descriptor_pool_reuses_and_grows():
+    import torch
+
+    from cutile.runtime import native
+    from cutile.runtime.serving import SolveKind, StencilServer
+
+    s = StencilServer([SolveKind("k", {}, 1)], device="cpu")
+    gsz = native.grid_size()
+    a = s._pool_alloc(2)
+    s._pool[a * gsz:(a + 2) * gsz] = 7
+    b = s._pool_alloc(3)
+    assert b == a + 2
+    s._pool_release(a, 2)
+    assert s._pool_alloc(2) == a            # a freed block of the same size comes back
+    blocks = [s._pool_alloc(3) for _ in range(200)]   # forces growth
+    assert len(set(blocks)) == 200
+    assert s._pool.numel() >= (max(blocks) + 3) * gsz
+    assert bool((s._pool[a * gsz:(a + 2) * gsz] == 7).all())   # contents survive growth
+    assert s._pool.dtype == torch.uint8
