@@ -318,3 +318,18 @@ def test_serving_descriptor_pool_reuses_and_grows():
     assert s._pool.numel() >= (max(blocks) + 3) * gsz
     assert bool((s._pool[a * gsz:(a + 2) * gsz] == 7).all())   # contents survive growth
     assert s._pool.dtype == torch.uint8
+
+
+def test_occupancy_hint_reaches_the_launch_bound():
+    from cutile import compile as stencil_compile
+    from cutile import stencil
+
+    fn = stencil(ndim=3)(D.lap7)
+    for occ in (1, 2, 4):
+        r = stencil_compile(fn, temporal_blocking=False, occupancy=occ)
+        bounds = re.findall(r"__launch_bounds__\((\d+), (\d+)\)", r.cuda_source)
+        assert bounds and all(int(b) == occ for _, b in bounds), (occ, bounds)
+        assert r.kernel_hints["occupancy"] == occ
+    # without a hint the planner derives it from shared memory and registers
+    r = stencil_compile(fn, temporal_blocking=False)
+    assert "occupancy" not in r.kernel_hints
