@@ -125,6 +125,38 @@ class StencilProgram:
                       scalars=self.scalar_values(scalars), red=out)
         return out
 
+    # -- graph-captured time loops --------------------------------------------
+    def capture_steps(self, set_a, set_b, steps: int, *, boundary: bool = False,
+                      scalars: dict | None = None):
+        """A CUDA graph of ``steps`` launches that ping-pong between two field
+        sets: step k reads set ``a`` (k even) or ``b`` and writes the other, so
+        after an even count the state is back in ``set_a``.  ``boundary``
+        launches the fused-boundary kernel (``step_<name>``).  Replay with
+        ``graph.replay()``; the launches are the eager ones, so results are
+        bit-identical to calling them in a loop."""
+        import torch
+
+        set_a, set_b = list(set_a), list(set_b)
+        nin, nout = self.spec["inputs"], self.spec["outputs"]
+        if len(set_a) != nin or len(set_b) != nin or nin != nout:
+            raise ValueError(f"{self.spec['name']}: a ping-pong loop needs as many outputs as "
+                             f"inputs and two sets of {nin} field(s)")
+        run = self.step if boundary else self.launch
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):       # load the module outside the capture
+            run(set_a, set_b, side, scalars=scalars)
+        side.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=side):
+            cur, nxt = set_a, set_b
+            for _ in range(steps):
+                run(cur, nxt, side, scalars=scalars)
+                cur, nxt = nxt, cur
+        # the graph holds raw addresses: keep the fields alive with it
+        graph.csd_fields = (tuple(set_a), tuple(set_b))
+        return graph
+
     # -- bricked layout ------------------------------------------------------
     def _brick(self, brick_size) -> int:
         bs = int(brick_size)
