@@ -178,10 +178,9 @@ def _align_up(x: int, a: int) -> int:
 
 
 def engine_geometry(plan: EnginePlan, radius3: tuple[int, int, int], dtype_bytes: int,
-                    num_inputs: int) -> dict:
-    """Derived sizes, identical to the constexprs of ``csd::Cfg`` (engine.cuh),
-    except ``smem_bytes``, which always counts the periodic wrap buffer (an
-    upper bound for the other boundary modes).
+                    num_inputs: int, periodic: bool = False) -> dict:
+    """Derived sizes, identical to the constexprs of ``csd::Cfg`` (engine.cuh);
+    ``periodic`` adds the periodic-X wrap buffer of fused periodic kernels.
 
     ``radius3`` is the radius of ONE stencil step per internal dimension
     (Z, Y, X); ``plan.temporal`` steps are chained.
@@ -205,7 +204,8 @@ def engine_geometry(plan: EnginePlan, radius3: tuple[int, int, int], dtype_bytes
     inter = sum(nslot_i * _align_up(plan.rows * (plan.tile_y + 2 * (T - s) * ry) * box_w, per128)
                 for s in range(1, T))
     wrapw = _align_up(rx, align) + align
-    pbuf_slot = num_inputs * 2 * _align_up(plan.rows * box_h * wrapw, per128) if rx > 0 else 0
+    pbuf_slot = (num_inputs * 2 * _align_up(plan.rows * box_h * wrapw, per128)
+                 if (periodic and rx > 0) else 0)
     smem = ((num_inputs * nslot * slot_elems + inter + nslot * pbuf_slot) * dtype_bytes
             + 8 * nslot + 64 + 128)
     return {"align": align, "pad_left": pad_left, "box_w": box_w, "box_h": box_h,
@@ -259,11 +259,11 @@ def radius3(ndim: int, radius: tuple[int, ...]) -> tuple[int, int, int]:
 
 
 def fit_plan(plan: EnginePlan, radius: tuple[int, ...], dtype_bytes: int,
-             num_inputs: int, body_ops: int = 0) -> EnginePlan:
+             num_inputs: int, body_ops: int = 0, periodic: bool = False) -> EnginePlan:
     """Shrink a plan until its TMA box and shared memory fit the B200 limits."""
     r3 = radius3(plan.ndim, radius)
     for _ in range(64):
-        g = engine_geometry(plan, r3, dtype_bytes, num_inputs)
+        g = engine_geometry(plan, r3, dtype_bytes, num_inputs, periodic)
         ok_box = g["box_w"] <= TMA_BOX_MAX and g["box_h"] <= TMA_BOX_MAX
         if ok_box and g["smem_bytes"] <= B200_SMEM_PER_BLOCK - 1024:
             break
@@ -283,7 +283,7 @@ def fit_plan(plan: EnginePlan, radius: tuple[int, ...], dtype_bytes: int,
         threads //= 2
     threads = max(32, threads)
     zchunk = 0 if plan.zchunk <= 0 else max(plan.rows, (plan.zchunk // plan.rows) * plan.rows)
-    g = engine_geometry(plan, r3, dtype_bytes, num_inputs)
+    g = engine_geometry(plan, r3, dtype_bytes, num_inputs, periodic)
     # resident blocks the shared memory allows, capped so the register budget
     # stays >= 64 per thread (128 for long bodies such as flux stencils, which
     # otherwise spill); the launch bound is a hint to ptxas, not a floor

@@ -475,7 +475,8 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
     kernels = {"main": name}
     if boundary_spec is not None:
         bc_plan = fit_plan(replace(plan, temporal=1), stencil_halo, dtype_bytes, num_inputs,
-                           analysis.get("body_ops", 0))
+                           analysis.get("body_ops", 0),
+                           periodic=boundary_spec.get("type") == "periodic")
         bc_target = lower_to_target_ir(ir.clone(), bc_plan.tile_sizes(), halo_widths,
                                        temporal_steps=1, boundary_spec=boundary_spec,
                                        kernel_hints=bc_plan.hints(), dtype=dtype,
@@ -624,8 +625,15 @@ def compile_fused(stencil_fns: list, domain: tuple[int, ...] | None = None, hw=N
     if boundary is not None:
         bspec = {"type": boundary} if isinstance(boundary, str) else (
             dict(boundary) if isinstance(boundary, dict) else boundary.to_dict())
-        bc_target = lower_fused_to_target_ir(modules, plan.tile_sizes(), tuple(halo_widths), hints,
-                                             dtype=dtype, boundary_mode=bspec["type"],
+        bc_hints = hints
+        if bspec["type"] == "periodic":
+            # the wrap buffer enlarges shared memory: refit the launch bound
+            bc_hints = fit_plan(plan, stencil_halo, dtype_bytes, meta.num_inputs, body_ops,
+                                periodic=True).hints()
+            if occupancy is not None:
+                bc_hints["occupancy"] = occupancy
+        bc_target = lower_fused_to_target_ir(modules, plan.tile_sizes(), tuple(halo_widths),
+                                             bc_hints, dtype=dtype, boundary_mode=bspec["type"],
                                              kahan=kahan)
         _rename_kernel(bc_target, f"{meta.name}_bc")
         cuda += "\n" + emit_cuda(bc_target, preamble=False)
@@ -697,10 +705,10 @@ def build_variants(stencil_fn, variants: dict, *, dtype: str | None = None,
                         + (m if rk.get("w") is not None else 0))
         plan = default_engine_plan(len(stencil_halo), num_loads, dtype_bytes, stencil_halo,
                                    n_fields + extra_in)
+        bmode = opts.pop("boundary_mode", "none")
         plan = fit_plan(_plan_from(tile_sizes, kernel_hints, len(stencil_halo), plan),
                         stencil_halo, dtype_bytes, n_fields + extra_in,
-                        analysis.get("body_ops", 0))
-        bmode = opts.pop("boundary_mode", "none")
+                        analysis.get("body_ops", 0), periodic=bmode == "periodic")
         target = lower_to_target_ir(ir.clone(), plan.tile_sizes(), tuple(halo_widths),
                                     kernel_hints=plan.hints(), dtype=dtype, name=kname,
                                     boundary_spec=bspec, boundary_mode=bmode, **opts)
