@@ -361,6 +361,26 @@ int csd_module_load(const char* src, int n_headers, const char* const* headers,
   return CSD_OK;
 }
 
+int csd_module_load_image(const void* image, size_t size, csd_module** out) {
+  if (!out || !image) return fail(CSD_EINVAL, "null argument");
+  // an ELF cubin starts with 0x7f 'E' 'L' 'F'; anything else (PTX text, a
+  // truncated file) is refused before the driver sees it
+  const unsigned char* b = static_cast<const unsigned char*>(image);
+  if (size < 64 || b[0] != 0x7f || b[1] != 'E' || b[2] != 'L' || b[3] != 'F')
+    return fail(CSD_EINVAL, "not a cubin image (%zu bytes)", size);
+  CUdevice dev;
+  int rc = ensure_context(&dev);
+  if (rc) return rc;
+  CUmodule mod;
+  CUresult r = drv().cuModuleLoadData(&mod, image);
+  if (r) return cu_fail(r, "cuModuleLoadData");
+  csd_module* m = new csd_module();
+  m->mod = mod;
+  m->dev = dev;
+  *out = m;
+  return CSD_OK;
+}
+
 int csd_module_unload(csd_module* m) {
   if (!m) return CSD_OK;
   if (m->mod && drv().ok) drv().cuModuleUnload(m->mod);

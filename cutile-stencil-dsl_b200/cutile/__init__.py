@@ -8,7 +8,7 @@ maximum, minimum, where`` (plus ``sqrt``).
 from cutile.frontend.decorator import stencil
 from cutile.frontend.elementwise import maximum, minimum, sqrt, where
 from cutile.frontend.types import BoundarySpec
-from cutile.runtime.launcher import compile, compile_fused
+from cutile.runtime.launcher import compile, compile_fused, load_aot
 from cutile.runtime.pipeline import Pipeline
 
 
@@ -20,5 +20,5 @@ def __getattr__(name):
     raise AttributeError(name)
 
 
-__all__ = ["stencil", "compile", "compile_fused", "Pipeline", "RKIntegrator", "BoundarySpec",
+__all__ = ["stencil", "compile", "compile_fused", "load_aot", "Pipeline", "RKIntegrator", "BoundarySpec",
            "maximum", "minimum", "where", "sqrt"]

@@ -37,6 +37,35 @@ from cutile.dialects.stencil import ApplyOp
 from cutile.runtime.pipeline import Pipeline
 
 
+def _import_file(path: str, module_name: str):
+    spec = importlib.util.spec_from_file_location(module_name, path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def load_aot(module_path: str):
+    """Import a launcher module written by ``CompileResult.build_aot``."""
+    import hashlib
+    import os
+
+    path = os.path.abspath(module_path)
+    name = os.path.splitext(os.path.basename(path))[0]
+    tag = hashlib.sha256(path.encode()).hexdigest()[:12]
+    return _import_file(path, f"_aot_{name}_{tag}")
+
+
+@dataclass
+class AotBuild:
+    """Paths of an ahead-of-time build and ptxas' resources per entry."""
+
+    cu: str
+    cubin: str
+    module: str
+    log: str
+    resources: dict = field(default_factory=dict)
+
+
 @dataclass
 class CompileResult:
     """Result of compiling a stencil (launcher.py:27-231)."""
@@ -80,11 +109,43 @@ class CompileResult:
         with tempfile.NamedTemporaryFile(suffix=".py", delete=False, mode="w") as f:
             f.write(self.code)
             tmp_path = f.name
-        spec = importlib.util.spec_from_file_location(f"_gen_{self.name}", tmp_path)
-        mod = importlib.util.module_from_spec(spec)
-        spec.loader.exec_module(mod)
-        self._module = mod
-        return mod
+        self._module = _import_file(tmp_path, f"_gen_{self.name}")
+        return self._module
+
+    def build_aot(self, directory: str, nvcc: str | None = None) -> "AotBuild":
+        """Ahead-of-time artefacts in ``directory``: ``<name>.cu`` (the CUDA
+        source, compilable on its own with ``-I`` the engine headers),
+        ``<name>.cubin`` (nvcc, sm_100a, the NVRTC path's flags) and
+        ``<name>.py``, the launcher module that loads that cubin instead of
+        compiling at first launch (same ``launch_<name>`` functions as
+        ``load_module()``).  Needs nvcc, not a GPU.  Mirrors the reference's
+        ``code`` / ``emit_to_file`` artefact (runtime/launcher.py:57-60)."""
+        import hashlib
+        import os
+        import re
+
+        from cutile.runtime import native
+        from cutile.runtime.regcheck import parse_ptxas_log
+
+        os.makedirs(directory, exist_ok=True)
+        cu = os.path.join(directory, f"{self.name}.cu")
+        cubin = os.path.join(directory, f"{self.name}.cubin")
+        shim = os.path.join(directory, f"{self.name}.py")
+        self.emit_cuda_to_file(cu)
+        log = native.aot_compile(cu, cubin, nvcc)
+        with open(cubin, "rb") as f:
+            digest = hashlib.sha256(f.read()).hexdigest()
+        code = self.code
+        if code.count(_CUBIN_LINE + "\n") != 1 or code.count(_CUBIN_HASH_LINE + "\n") != 1:
+            raise RuntimeError(f"{self.name}: generated module has no cubin slot")
+        code = code.replace(_CUBIN_LINE + "\n", "CUBIN = os.path.join(os.path.dirname("
+                            f"os.path.abspath(__file__)), {os.path.basename(cubin)!r})\n")
+        code = code.replace(_CUBIN_HASH_LINE + "\n", f"CUBIN_SHA256 = {digest!r}\n")
+        with open(shim, "w") as f:
+            f.write(code)
+        entries = re.findall(r"Compiling entry function '([^']+)'", log)
+        return AotBuild(cu=cu, cubin=cubin, module=shim, log=log,
+                        resources={n: parse_ptxas_log(log, n) for n in entries})
 
     # -- self checks ---------------------------------------------------------
     def _np_dtype(self):
@@ -282,6 +343,18 @@ def _plan_from(tile_sizes, kernel_hints, ndim, base_plan):
     return p
 
 
+# The generated module's program lines.  An ahead-of-time build rewrites the
+# two ``None`` lines to name the cubin beside the module and its hash.
+_CUBIN_LINE = "CUBIN = None"
+_CUBIN_HASH_LINE = "CUBIN_SHA256 = None"
+
+
+def _program_lines(e) -> None:
+    e.line(_CUBIN_LINE)
+    e.line(_CUBIN_HASH_LINE)
+    e.line("_PROGRAM = StencilProgram(CUDA_SOURCE, SPEC, cubin=CUBIN, cubin_sha256=CUBIN_SHA256)")
+
+
 def generate_module_code(name: str, cuda_source: str, spec: dict, *, fused_outputs=None) -> str:
     """Python launcher module around ``cuda_source`` (the ``code`` of a result)."""
     from cutile.lowering.emitter import CodeEmitter
@@ -289,13 +362,15 @@ def generate_module_code(name: str, cuda_source: str, spec: dict, *, fused_outpu
     e = CodeEmitter()
     e.line(f'"""B200 stencil module for {name} (generated)."""')
     e.blank()
+    e.line("import os")
+    e.blank()
     e.line("from cutile.runtime.module import StencilProgram")
     e.blank()
     e.line("CUDA_SOURCE = r'''" + cuda_source + "'''")
     e.blank()
     e.line(f"SPEC = {spec!r}")
     e.line("SPEC['halo'] = tuple(SPEC['halo'])")
-    e.line("_PROGRAM = StencilProgram(CUDA_SOURCE, SPEC)")
+    _program_lines(e)
     inputs = spec["input_names"]
     outs = spec["output_params"]
     scal = spec.get("scalars", [])
@@ -742,12 +817,14 @@ def _compile_reduction(stencil_fn, reduce: str, *, dtype=None, precision=None,
     e = CodeEmitter()
     e.line(f'"""Per-grid max of {name} over the interior (generated)."""')
     e.blank()
+    e.line("import os")
+    e.blank()
     e.line("from cutile.runtime.module import StencilProgram")
     e.blank()
     e.line("CUDA_SOURCE = r\'\'\'" + cuda + "\'\'\'")
     e.line(f"SPEC = {spec!r}")
     e.line("SPEC['halo'] = tuple(SPEC['halo'])")
-    e.line("_PROGRAM = StencilProgram(CUDA_SOURCE, SPEC)")
+    _program_lines(e)
     e.blank()
     e.blank()
     e.line(f"def reduce_{name}({', '.join(names)}, out=None, stream=None, **scalars):")

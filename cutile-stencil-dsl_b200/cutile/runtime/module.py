@@ -27,9 +27,14 @@ class StencilProgram:
     ``main`` and optionally ``fused_bc``), ``zchunk``.
     """
 
-    def __init__(self, cuda_source: str, spec: dict):
+    def __init__(self, cuda_source: str, spec: dict, cubin: str | None = None,
+                 cubin_sha256: str | None = None):
         self.source = cuda_source
         self.spec = dict(spec)
+        # a prebuilt cubin of ``cuda_source`` (ahead-of-time build) replaces the
+        # NVRTC compile; it is checked against its recorded hash at load
+        self.cubin = cubin
+        self.cubin_sha256 = cubin_sha256
         self._modules: dict[int, native.NativeModule] = {}
         self._lock = threading.Lock()
 
@@ -44,7 +49,11 @@ class StencilProgram:
             m = self._modules.get(dev)
             if m is None:
                 torch.cuda.init()
-                m = native.NativeModule(self.source)
+                if self.cubin is not None:
+                    m = native.NativeModule(self.source, image=native.read_image(
+                        self.cubin, self.cubin_sha256))
+                else:
+                    m = native.NativeModule(self.source)
                 self._modules[dev] = m
         return m
 

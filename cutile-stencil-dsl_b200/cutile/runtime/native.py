@@ -91,6 +91,7 @@ def library() -> ctypes.CDLL:
         lib.csd_compile.argtypes = [cp, ctypes.c_int, ctypes.POINTER(cp), ctypes.POINTER(cp), cp, cp,
                                     ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p,
                                     ctypes.c_size_t]
+        lib.csd_module_load_image.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(P)]
         lib.csd_module_unload.argtypes = [P]
         lib.csd_kernel_get.argtypes = [P, cp, ctypes.POINTER(P)]
         lib.csd_kernel_describe.argtypes = [P, ctypes.POINTER(KernelDesc)]
@@ -163,15 +164,79 @@ def compile_source(src: str, extra_options=()) -> tuple[str, str]:
     return path.value.decode(), log.value.decode(errors="replace")
 
 
-class NativeModule:
-    """A loaded JIT module (per CUDA context)."""
+# nvcc flags equivalent to NVRTC_OPTIONS for ahead-of-time builds of the same
+# source (nvcc has no -default-device; the engine headers mark every device
+# function themselves).
+NVCC_OPTIONS = (
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-cubin",
+    "-std=c++17",
+    "-fmad=false",
+    "-DNDEBUG",
+    "-lineinfo",
+    "-Xptxas", "-v",
+)
 
-    def __init__(self, src: str, extra_options=()):
+
+def find_nvcc() -> str:
+    """nvcc from ``CUDA_HOME``/``CUDA_PATH``, then ``PATH``, then /usr/local/cuda."""
+    import shutil
+
+    for env in ("CUDA_HOME", "CUDA_PATH"):
+        root = os.environ.get(env)
+        if root and os.path.exists(os.path.join(root, "bin", "nvcc")):
+            return os.path.join(root, "bin", "nvcc")
+    found = shutil.which("nvcc")
+    if found:
+        return found
+    if os.path.exists("/usr/local/cuda/bin/nvcc"):
+        return "/usr/local/cuda/bin/nvcc"
+    raise CsdError("nvcc not found (set CUDA_HOME); ahead-of-time builds need the CUDA toolkit")
+
+
+def aot_compile(cu_path: str, cubin_path: str, nvcc: str | None = None) -> str:
+    """Compile a generated module's ``.cu`` to an sm_100a cubin with nvcc (no
+    GPU needed); returns nvcc's log (the ptxas ``-v`` resource report)."""
+    import subprocess
+
+    cmd = [nvcc or find_nvcc(), *NVCC_OPTIONS, "-I", str(INCLUDE_DIR), cu_path, "-o", cubin_path]
+    proc = subprocess.run(cmd, capture_output=True, text=True)
+    log = proc.stdout + proc.stderr
+    if proc.returncode != 0:
+        raise CsdError(f"nvcc failed ({proc.returncode}): {' '.join(cmd)}\n{log}")
+    return log
+
+
+def read_image(path: str, sha256: str | None = None) -> bytes:
+    """Bytes of a prebuilt cubin, checked against ``sha256`` when given (a
+    cubin rebuilt or replaced after its launcher module was written is
+    refused rather than launched with a stale kernel contract)."""
+    import hashlib
+
+    if not os.path.exists(path):
+        raise CsdError(f"prebuilt cubin {path} is missing")
+    with open(path, "rb") as f:
+        data = f.read()
+    if sha256 is not None and hashlib.sha256(data).hexdigest() != sha256:
+        raise CsdError(f"prebuilt cubin {path} does not match its launcher module "
+                       f"(sha256 differs): rebuild it with CompileResult.build_aot")
+    return data
+
+
+class NativeModule:
+    """A loaded module (per CUDA context): JIT-compiled from ``src`` with
+    NVRTC, or, given ``image``, a prebuilt cubin of the same source."""
+
+    def __init__(self, src: str, extra_options=(), image: bytes | None = None):
         lib = library()
-        n, hdrs, names = _headers()
         handle = ctypes.c_void_p()
-        check(lib.csd_module_load(src.encode(), n, hdrs, names, _options(extra_options),
-                                  default_cache_dir().encode(), ctypes.byref(handle)))
+        if image is not None:
+            buf = ctypes.create_string_buffer(image, len(image))
+            check(lib.csd_module_load_image(buf, len(image), ctypes.byref(handle)))
+        else:
+            n, hdrs, names = _headers()
+            check(lib.csd_module_load(src.encode(), n, hdrs, names, _options(extra_options),
+                                      default_cache_dir().encode(), ctypes.byref(handle)))
         self.handle = handle
         self._kernels: dict[str, NativeKernel] = {}
 
@@ -405,4 +470,4 @@ __all__ = ["library", "check", "compile_source", "NativeModule", "NativeKernel",
            "apply_boundary", "error_word", "CsdError", "field_of", "default_cache_dir",
            "make_opts", "grid_size", "grid_build", "launch_batch", "bricked_shape",
            "to_bricks", "from_bricks", "bricked_field", "launch_fields",
-           "CSD_LOADER_TMA", "CSD_LOADER_LDG", "BC_MODES"]
+           "NVCC_OPTIONS", "find_nvcc", "aot_compile", "read_image", "CSD_LOADER_TMA", "CSD_LOADER_LDG", "BC_MODES"]

@@ -56,9 +56,10 @@ def parse_ptxas_log(text: str, entry: str | None = None) -> Optional[Resources]:
         if entry is not None and name != entry:
             continue
         regs = re.search(r"Used (\d+) registers", blk)
+        # NVRTC prefixes the frame line with "ptxas ."; nvcc's report does not
         frame = re.search(r"Function properties for " + re.escape(name) +
-                          r"\s*\n\s*ptxas\s+\.\s+(\d+) bytes stack frame, (\d+) bytes spill stores",
-                          blk)
+                          r"\s*\n\s*(?:ptxas\s+\.\s+)?(\d+) bytes stack frame, "
+                          r"(\d+) bytes spill stores", blk)
         if regs is None:
             continue
         stack = int(frame.group(1)) if frame else 0

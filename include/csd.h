@@ -92,6 +92,14 @@ int csd_compile(const char* src, int n_headers, const char* const* headers,
                 const char* const* header_names, const char* options, const char* cache_dir,
                 char* cubin_path, size_t path_len, char* log, size_t log_len);
 
+/* Load a prebuilt sm_100a cubin (`image`, `size` bytes) into the current
+ * device's primary context: the ahead-of-time form of csd_module_load, for a
+ * generated module compiled by nvcc from the `.cu` that
+ * CompileResult.build_aot writes.  Stands in for loading the artefact of the
+ * reference's `CompileResult.code` / `emit_to_file` (runtime/launcher.py:57-60)
+ * without a JIT at first launch. */
+int csd_module_load_image(const void* image, size_t size, csd_module** out);
+
 int csd_module_unload(csd_module* m);
 
 /* Look up stencil kernel `name` (its `<name>_tma`, `<name>_ldg` entry points
