@@ -489,6 +489,94 @@ static bool row_pitched(const csd_field& f) {
 }
 
 // Validate one grid's fields and fill its kernel-side descriptor.
+// Cut a column of `nz` rows into about `cnt` items of a multiple of `rows`
+// rows each; with `shift`, the first and last item are about 4 % shorter
+// than the others (zs rows).  Returns the number of items, every one
+// non-empty: item tz covers [tz*zc - zs, (tz+1)*zc - zs) clipped to [0, nz).
+static long long split_column(long long nz, long long cnt, int rows, bool shift, int* zc,
+                              int* zs) {
+  if (cnt < 1) cnt = 1;
+  long long s = shift && cnt >= 2 ? (nz / cnt) / 24 / rows * rows : 0;
+  long long z = ((nz + 2 * s + cnt - 1) / cnt + rows - 1) / rows * rows;
+  long long n = (nz + s + z - 1) / z;
+  if (s > 0 && (z <= s || n < 2)) {
+    s = 0;
+    z = ((nz + cnt - 1) / cnt + rows - 1) / rows * rows;
+    n = (nz + z - 1) / z;
+  }
+  *zc = (int)z;
+  *zs = (int)s;
+  return n;
+}
+
+int csd_plan_items(const csd_kernel_desc* D, long long slots, int zchunk_req, csd_grid* g) {
+  if (!D || !g) return fail(CSD_EINVAL, "null argument");
+  if (D->rows < 1 || g->tiles[0] < 1 || g->tiles[1] < 1 || g->interior[0] < 1)
+    return fail(CSD_EINVAL, "empty work split");
+  // Work items (column tiles x Z chunks) sized so that they fill the
+  // resident CTAs in one wave: items of equal length that start together
+  // keep neighbouring columns on the same planes (their halo rows are then
+  // shared in L2) and leave no tail.
+  const long long nz = g->interior[0];
+  const int rows = D->rows;
+  const long long columns = (long long)g->tiles[0] * g->tiles[1];
+  int zchunk = zchunk_req > 0 ? zchunk_req : D->zchunk;
+  const bool one_wave = zchunk_req <= 0 && D->zchunk == 0;
+  if (zchunk <= 0) {
+    // -W: W items per resident block (issue-bound bodies balance better)
+    const long long waves = zchunk < 0 ? -(long long)zchunk : 1;
+    long long nzc = slots * waves / (columns > 0 ? columns : 1);
+    if (nzc < 1) nzc = 1;
+    if (nzc > nz) nzc = nz;
+    zchunk = (int)((nz + nzc - 1) / nzc);
+  }
+  g->zchunk = ((zchunk + rows - 1) / rows) * rows;
+  if (g->zchunk > nz) g->zchunk = (int)(((nz + rows - 1) / rows) * rows);
+  g->tiles[2] = (int)((nz + g->zchunk - 1) / g->zchunk);
+  g->ecols = 0;
+  g->zshift = g->zshift_e = 0;
+  g->zchunk_e = g->zchunk;
+  long long items = columns * g->tiles[2];
+  // A fused boundary fill makes the X-edge columns and every column's first
+  // and last item slower than the rest (their chunks are patched); in a
+  // one-wave split the kernel lasts as long as its slowest item, so those
+  // items are made shorter: the X-edge columns take ~1.25x as many items
+  // from the wave's unused slots, and first/last items give up ~4 % of rows.
+  if (D->bc_mode != CSD_BC_NONE && one_wave) {
+    const long long spare = slots - items;
+    int zc, zs;
+    const long long n = split_column(nz, g->tiles[2], rows, true, &zc, &zs);
+    g->tiles[2] = (int)n;
+    g->zchunk = g->zchunk_e = zc;
+    g->zshift = g->zshift_e = zs;
+    items = columns * n;
+    const long long ncol_e = 2ll * g->tiles[1];
+    long long ne = n + (n + 3) / 4;
+    if ((ne - n) * ncol_e > spare) ne = n + (spare > 0 ? spare / ncol_e : 0);
+    if (ne > nz / rows) ne = nz / rows;
+    if (g->tiles[0] >= 3 && ne > n) {
+      ne = split_column(nz, ne, rows, true, &zc, &zs);
+      if (ne > n) {
+        g->ecols = 2;
+        g->items_main = (int)((long long)(g->tiles[0] - 2) * g->tiles[1] * n);
+        g->zchunk_e = zc;
+        g->zshift_e = zs;
+        items = g->items_main + ncol_e * ne;
+      }
+    }
+  }
+  if (items > 0x7fffffff) return fail(CSD_EINVAL, "too many work items");
+  g->items = (int)items;
+  return CSD_OK;
+}
+
+int csd_grid_item_place(const csd_grid* g, int item, int* tx, int* ty, int* z0, int* nrows) {
+  if (!g || !tx || !ty || !z0 || !nrows) return fail(CSD_EINVAL, "null argument");
+  if (item < 0 || item >= g->items) return fail(CSD_EINVAL, "item %d out of [0, %d)", item, g->items);
+  csd_item_place(g, item, tx, ty, z0, nrows);
+  return CSD_OK;
+}
+
 static int build_grid(csd_kernel* k, const csd_field* in, int n_in, const csd_field* out,
                       int n_out, const csd_launch_opts& o, DeviceState* st, int loader_req,
                       csd_grid* g, int* loader_out) {
@@ -570,27 +658,9 @@ static int build_grid(csd_kernel* k, const csd_field* in, int n_in, const csd_fi
   if (loader < 0 || loader > 1) loader = tma_ok ? CSD_LOADER_TMA : CSD_LOADER_LDG;
   if (loader == CSD_LOADER_TMA && !tma_ok)
     return fail(CSD_EALIGN, "TMA path needs 16-byte aligned fields and row pitch");
-  // Work items (column tiles x Z chunks) sized so that they fill the
-  // resident CTAs in one wave: items of equal length that start together
-  // keep neighbouring columns on the same planes (their halo rows are then
-  // shared in L2) and leave no tail.
   const long long slots = o.grid > 0 ? o.grid : (long long)k->blocks_per_sm[loader] * st->sms;
-  const long long columns = (long long)g->tiles[0] * g->tiles[1];
-  int zchunk = o.zchunk > 0 ? o.zchunk : D.zchunk;
-  if (zchunk <= 0) {
-    // -W: W items per resident block (issue-bound bodies balance better)
-    const long long waves = zchunk < 0 ? -(long long)zchunk : 1;
-    long long nzc = slots * waves / (columns > 0 ? columns : 1);
-    if (nzc < 1) nzc = 1;
-    if (nzc > g->interior[0]) nzc = g->interior[0];
-    zchunk = (int)((g->interior[0] + nzc - 1) / nzc);
-  }
-  g->zchunk = ((zchunk + D.rows - 1) / D.rows) * D.rows;
-  if (g->zchunk > g->interior[0]) g->zchunk = ((g->interior[0] + D.rows - 1) / D.rows) * D.rows;
-  g->tiles[2] = (g->interior[0] + g->zchunk - 1) / g->zchunk;
-  long long items = columns * g->tiles[2];
-  if (items > 0x7fffffff) return fail(CSD_EINVAL, "too many work items");
-  g->items = (int)items;
+  int rc = csd_plan_items(&D, slots, o.zchunk, g);
+  if (rc) return rc;
   g->bc_value = o.bc_value;
   for (int i = 0; i < CSD_MAX_SCALARS; ++i) g->scalars[i] = o.scalars[i];
   for (int i = 0; i < CSD_MAX_FIELDS; ++i) g->bc_odd[i] = o.bc_odd[i];

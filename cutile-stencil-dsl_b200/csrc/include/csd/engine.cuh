@@ -388,19 +388,66 @@ __device__ __forceinline__ void patch_cell(const csd_grid& g, typename C::T* rin
   const int hz = g.halo[0], hy = g.halo[1], hx = g.halo[2];
   const int nz = g.interior[0], ny = g.interior[1], nx = g.interior[2];
   const bool out_x = (gx < hx || gx >= hx + nx) && g.dims[2] > 1;
+  // every field's value is loaded before the first store (see patch_line)
+  T v[C::NIN];
+  if (C::BC == CSD_BC_DIRICHLET) {
+#pragma unroll
+    for (int f = 0; f < C::NIN; ++f) v[f] = (T)g.bc_value;
+  } else {
+    const long long mx = out_x ? bc_map(gx, hx, nx, C::BC) : gx;
+    const long long my = out_y ? bc_map(gy, hy, ny, C::BC) : gy;
+    const long long mz = out_z ? bc_map(gz, hz, nz, C::BC) : gz;
+    const long long off = elem_off<C>(g, mz, my, mx);
+#pragma unroll
+    for (int f = 0; f < C::NIN; ++f) {
+      v[f] = __ldg(reinterpret_cast<const T*>(g.in[f]) + off);
+      if (C::BC == CSD_BC_REFLECTING && odd_flip<C>(g, f, out_x, out_y, out_z)) v[f] = -v[f];
+    }
+  }
+#pragma unroll
+  for (int f = 0; f < C::NIN; ++f) ring[(f * C::NSLOT + slot) * C::SLOT_ELEMS + e] = v[f];
+}
+
+// A whole line outside the interior in Z or Y, from global memory.  Per
+// field, each lane issues all of its loads before any store: the stores go
+// to shared memory through a generic pointer that the compiler cannot tell
+// apart from the loads' global memory, so interleaved loads and stores would
+// pay the global latency once per cell.
+template <class C>
+__device__ __forceinline__ void patch_line(const csd_grid& g, typename C::T* ring, int slot,
+                                           int line, int x0, int xa, int xb, long long gy,
+                                           long long gz, bool out_y, bool out_z, int lane) {
+  typedef typename C::T T;
+  constexpr int MAXC = (C::BOXW + 31) / 32;
+  const int hz = g.halo[0], hy = g.halo[1], hx = g.halo[2];
+  const int nz = g.interior[0], ny = g.interior[1], nx = g.interior[2];
+  const long long my = out_y ? bc_map(gy, hy, ny, C::BC) : gy;
+  const long long mz = out_z ? bc_map(gz, hz, nz, C::BC) : gz;
 #pragma unroll
   for (int f = 0; f < C::NIN; ++f) {
-    T v;
-    if (C::BC == CSD_BC_DIRICHLET) {
-      v = (T)g.bc_value;
-    } else {
-      const long long mx = out_x ? bc_map(gx, hx, nx, C::BC) : gx;
-      const long long my = out_y ? bc_map(gy, hy, ny, C::BC) : gy;
-      const long long mz = out_z ? bc_map(gz, hz, nz, C::BC) : gz;
-      v = reinterpret_cast<const T*>(g.in[f])[elem_off<C>(g, mz, my, mx)];
-      if (C::BC == CSD_BC_REFLECTING && odd_flip<C>(g, f, out_x, out_y, out_z)) v = -v;
+    T v[MAXC];
+    T* dst = ring + (f * C::NSLOT + slot) * C::SLOT_ELEMS + line * C::BOXW;
+#pragma unroll
+    for (int c = 0; c < MAXC; ++c) {
+      const int xx = xa + lane + 32 * c;
+      v[c] = T(0);
+      if (xx < xb) {
+        const long long gx = (long long)x0 + xx;
+        const bool out_x = (gx < hx || gx >= hx + nx) && g.dims[2] > 1;
+        if (C::BC == CSD_BC_DIRICHLET) {
+          v[c] = (T)g.bc_value;
+        } else {
+          const long long mx = out_x ? bc_map(gx, hx, nx, C::BC) : gx;
+          v[c] = __ldg(reinterpret_cast<const T*>(g.in[f]) + elem_off<C>(g, mz, my, mx));
+          if (C::BC == CSD_BC_REFLECTING && odd_flip<C>(g, f, out_x, out_y, out_z)) v[c] = -v[c];
+        }
+      }
     }
-    ring[(f * C::NSLOT + slot) * C::SLOT_ELEMS + e] = v;
+#pragma unroll
+    for (int c = 0; c < MAXC; ++c) {
+      const int xx = xa + lane + 32 * c;
+      if (xx < xb) dst[xx] = v[c];
+    }
   }
 }
 
@@ -422,18 +469,21 @@ __device__ __forceinline__ void patch_x_cell(const csd_grid& g, typename C::T* r
   const int sx = (int)(src - x0);  // source box column (same line)
   // periodic: column of the source in its wrap block
   const int wx = C::PBUF ? (int)(src - Loader<C>::wrap_x(g, side)) : 0;
+  // sources of all fields first, then the stores (see patch_line)
+  T v[C::NIN];
 #pragma unroll
   for (int f = 0; f < C::NIN; ++f) {
-    T* slot_base = ring + (f * C::NSLOT + slot) * C::SLOT_ELEMS;
-    T v;
+    const T* slot_base = ring + (f * C::NSLOT + slot) * C::SLOT_ELEMS;
     if (C::BC == CSD_BC_PERIODIC) {
-      v = pbuf[(f * 2 + side) * C::WRAP_BLOCK + line * C::WRAPW + wx];
+      v[f] = pbuf[(f * 2 + side) * C::WRAP_BLOCK + line * C::WRAPW + wx];
     } else {
-      v = slot_base[line * C::BOXW + sx];
-      if (C::BC == CSD_BC_REFLECTING && odd_flip<C>(g, f, true, false, false)) v = -v;
+      v[f] = slot_base[line * C::BOXW + sx];
+      if (C::BC == CSD_BC_REFLECTING && odd_flip<C>(g, f, true, false, false)) v[f] = -v[f];
     }
-    slot_base[line * C::BOXW + xx] = v;
   }
+#pragma unroll
+  for (int f = 0; f < C::NIN; ++f)
+    ring[(f * C::NSLOT + slot) * C::SLOT_ELEMS + line * C::BOXW + xx] = v[f];
 }
 
 template <class C>
@@ -466,8 +516,7 @@ __device__ __forceinline__ void patch_boundary(const csd_grid& g, typename C::T*
     const bool out_y = (gy < hy || gy >= hy + ny) && g.dims[1] > 1;
     const bool out_z = (gz < hz || gz >= hz + nz) && g.dims[0] > 1;
     if (out_y || out_z) {
-      for (int xx = xa + lane; xx < xb; xx += 32)
-        patch_cell<C>(g, ring, slot, line * C::BOXW + xx, (long long)x0 + xx, gy, gz, out_y, out_z);
+      patch_line<C>(g, ring, slot, line, x0, xa, xb, gy, gz, out_y, out_z, lane);
     } else {
       // left: [xa, hx - x0), right: [hx + nx - x0, xb)
       const int l1 = min(xb, hx - x0);
@@ -557,14 +606,10 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
     const csd_grid& g = BATCHED ? p.grids[batch_grid_of(p, gitem, item)] : p.g;
     const int hz = g.halo[0], hy = g.halo[1], hx = g.halo[2];
     const int nz = g.interior[0], ny = g.interior[1], nx = g.interior[2];
-    const int tx = item % g.tiles[0];
-    const int t1 = item / g.tiles[0];
-    const int ty = t1 % g.tiles[1];
-    const int tz = t1 / g.tiles[1];
+    int tx, ty, z0, nrows;
+    csd_item_place(&g, item, &tx, &ty, &z0, &nrows);
     const int X0 = g.xbase + tx * C::TX;  // array column of the tile's first point
     const int Y0 = hy + ty * C::TY;
-    const int z0 = tz * g.zchunk;         // interior row of the item's first output row
-    const int nrows = min(g.zchunk, nz - z0);
     const int nsteps = cdiv(nrows, C::ROWS);
     const int nchunks = nsteps + 2 * HCT;
     // array coordinates of input chunk 0

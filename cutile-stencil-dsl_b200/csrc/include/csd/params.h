@@ -6,7 +6,7 @@
 
 #define CSD_MAX_FIELDS 8
 #define CSD_MAX_SCALARS 8
-#define CSD_DESC_MAGIC 0x43534432u /* "CSD2" */
+#define CSD_DESC_MAGIC 0x43534433u /* "CSD3": bumped with every csd_grid layout change */
 
 #define CSD_LOADER_TMA 0
 #define CSD_LOADER_LDG 1
@@ -46,6 +46,18 @@ typedef struct __attribute__((aligned(64))) csd_grid {
   int xbase;                          // X origin of tile 0 (halo rounded down to 16 B)
   int vec_store;                      // 1 when 16-byte output stores are aligned
   int ndim;                           // array dimensionality (1-3)
+  // Uneven work split of fused-boundary kernels.  Chunks of an X-edge column
+  // also take the boundary patch, so with ecols == 2 the two X-edge columns
+  // get their own, shorter items (item numbers items_main onward, zchunk_e
+  // rows); and the first and last item of a column, which patch the Z
+  // boundary, are zshift (zshift_e) rows shorter than the others: item tz of
+  // a column covers interior rows [tz*zc - zs, (tz+1)*zc - zs) clipped to
+  // [0, nz).  ecols == 0 and zshift == 0 give the uniform split.
+  int ecols;
+  int items_main;
+  int zchunk_e;
+  int zshift;
+  int zshift_e;
   double scalars[CSD_MAX_SCALARS];    // per-grid constants read by the body (s<k>)
   const double* dyn;                  // per-grid device scalars (d<k>), may be null
   double* red;                        // per-grid max-reduction slot, may be null
@@ -60,6 +72,34 @@ typedef struct __attribute__((aligned(64))) csd_grid {
   // rows) of the inputs, loaded from the far side of a row for X-edge chunks.
   csd_tmap tmap_wrap[CSD_MAX_FIELDS];
 } csd_grid;
+
+#if defined(__CUDACC__) || defined(__CUDACC_RTC__)
+#define CSD_HOST_DEVICE __host__ __device__ __forceinline__
+#else
+#define CSD_HOST_DEVICE static inline
+#endif
+
+// Column (tx, ty) and interior Z rows [z0, z0 + nrows) of work item `item` of
+// grid `g` (the split is described at csd_grid::ecols).  The kernels and the
+// host (csd_grid_item_place) decode items with this one function.
+CSD_HOST_DEVICE void csd_item_place(const csd_grid* g, int item, int* tx, int* ty, int* z0,
+                                    int* nrows) {
+  const int edge = g->ecols != 0 && item >= g->items_main;
+  const int c = edge ? item - g->items_main : item;
+  const int w = g->ecols == 0 ? g->tiles[0] : (edge ? 2 : g->tiles[0] - 2);
+  const int zc = edge ? g->zchunk_e : g->zchunk;
+  const int zs = edge ? g->zshift_e : g->zshift;
+  const int cx = c % w;
+  const int t1 = c / w;
+  const int tz = t1 / g->tiles[1];
+  int lo = tz * zc - zs, hi = (tz + 1) * zc - zs;
+  if (lo < 0) lo = 0;
+  if (hi > g->interior[0]) hi = g->interior[0];
+  *ty = t1 % g->tiles[1];
+  *tx = edge ? (cx ? g->tiles[0] - 1 : 0) : cx + (g->ecols ? 1 : 0);
+  *z0 = lo;
+  *nrows = hi - lo;
+}
 
 // Kernel parameter: one grid inline, or a device array of grids.
 typedef struct __attribute__((aligned(64))) csd_params {

@@ -67,6 +67,20 @@ class KernelDesc(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class GridHead(ctypes.Structure):
+    """The leading fields of ``csd_grid`` up to its work split (the TMA maps
+    and pointers before them are opaque here)."""
+
+    _fields_ = [("tmap", ctypes.c_ubyte * (128 * 8)), ("inp", ctypes.c_void_p * 8),
+                ("out", ctypes.c_void_p * 8), ("dims", ctypes.c_longlong * 3),
+                ("pitch_y", ctypes.c_longlong), ("pitch_z", ctypes.c_longlong),
+                ("halo", ctypes.c_int * 3), ("interior", ctypes.c_int * 3),
+                ("tiles", ctypes.c_int * 3), ("items", ctypes.c_int), ("zchunk", ctypes.c_int),
+                ("xbase", ctypes.c_int), ("vec_store", ctypes.c_int), ("ndim", ctypes.c_int),
+                ("ecols", ctypes.c_int), ("items_main", ctypes.c_int), ("zchunk_e", ctypes.c_int),
+                ("zshift", ctypes.c_int), ("zshift_e", ctypes.c_int)]
+
+
 _lib = None
 _lib_lock = threading.Lock()
 
@@ -92,6 +106,10 @@ def library() -> ctypes.CDLL:
                                     ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p,
                                     ctypes.c_size_t]
         lib.csd_module_load_image.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(P)]
+        lib.csd_plan_items.argtypes = [ctypes.POINTER(KernelDesc), ctypes.c_longlong, ctypes.c_int,
+                                       ctypes.c_void_p]
+        pi = ctypes.POINTER(ctypes.c_int)
+        lib.csd_grid_item_place.argtypes = [ctypes.c_void_p, ctypes.c_int, pi, pi, pi, pi]
         lib.csd_module_unload.argtypes = [P]
         lib.csd_kernel_get.argtypes = [P, cp, ctypes.POINTER(P)]
         lib.csd_kernel_describe.argtypes = [P, ctypes.POINTER(KernelDesc)]
@@ -340,6 +358,29 @@ def grid_size() -> int:
     return int(library().csd_grid_size())
 
 
+def plan_items(desc: dict, tiles_x: int, tiles_y: int, nz: int, slots: int,
+               zchunk: int = 0) -> tuple[dict, list]:
+    """The work split ``csd_launch`` uses for a grid of ``tiles_x x tiles_y``
+    columns and ``nz`` interior rows on ``slots`` resident CTAs (host only):
+    the split fields and every item's ``(tx, ty, z0, nrows)``."""
+    lib = library()
+    kd = KernelDesc(**{k: v for k, v in desc.items() if k in dict(KernelDesc._fields_)})
+    buf = ctypes.create_string_buffer(grid_size())
+    head = GridHead.from_buffer(buf)
+    head.tiles[0], head.tiles[1] = tiles_x, tiles_y
+    head.interior[0] = nz
+    check(lib.csd_plan_items(ctypes.byref(kd), slots, zchunk, ctypes.addressof(buf)))
+    split = {k: getattr(head, k) for k in ("items", "zchunk", "ecols", "items_main", "zchunk_e",
+                                           "zshift", "zshift_e")}
+    split["tiles_z"] = head.tiles[2]
+    out = []
+    v = [ctypes.c_int() for _ in range(4)]
+    for i in range(head.items):
+        check(lib.csd_grid_item_place(ctypes.addressof(buf), i, *[ctypes.byref(x) for x in v]))
+        out.append(tuple(x.value for x in v))
+    return split, out
+
+
 def grid_build(kernel: NativeKernel, inputs, outputs, halo, dest, **kw) -> tuple[int, int]:
     """Write the descriptor of one batched grid into host buffer ``dest``
     (a ctypes buffer of ``grid_size()`` bytes); returns (work items, loader)."""
@@ -470,4 +511,4 @@ __all__ = ["library", "check", "compile_source", "NativeModule", "NativeKernel",
            "apply_boundary", "error_word", "CsdError", "field_of", "default_cache_dir",
            "make_opts", "grid_size", "grid_build", "launch_batch", "bricked_shape",
            "to_bricks", "from_bricks", "bricked_field", "launch_fields",
-           "NVCC_OPTIONS", "find_nvcc", "aot_compile", "read_image", "CSD_LOADER_TMA", "CSD_LOADER_LDG", "BC_MODES"]
+           "GridHead", "plan_items", "NVCC_OPTIONS", "find_nvcc", "aot_compile", "read_image", "CSD_LOADER_TMA", "CSD_LOADER_LDG", "BC_MODES"]

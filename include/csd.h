@@ -133,6 +133,19 @@ int csd_launch(csd_kernel* k, const csd_field* in, int n_in, const csd_field* ou
 int csd_grid_build(csd_kernel* k, const csd_field* in, int n_in, const csd_field* out, int n_out,
                    const csd_launch_opts* opts, csd_grid* g, int* items, int* loader_used);
 
+/* Work split of grid `g` (tiles[0], tiles[1] and interior[0] set) for kernel
+ * `desc` on `slots` resident CTAs: sets zchunk, tiles[2], items and, for
+ * fused-boundary kernels sized for one wave, the uneven split described at
+ * csd_grid::ecols.  `zchunk_req` > 0 forces the rows per item.  Host only
+ * (csd_launch and csd_grid_build call it).  Replaces the reference's
+ * `_fit_tiles` grid sizing (target_to_python.py:305-348). */
+int csd_plan_items(const csd_kernel_desc* desc, long long slots, int zchunk_req, csd_grid* g);
+
+/* Host decode of work item `item` of a planned grid: column (tx, ty) and the
+ * interior Z rows [z0, z0 + nrows) it writes (the kernels use the same
+ * function, csd_item_place).  No reference counterpart. */
+int csd_grid_item_place(const csd_grid* g, int item, int* tx, int* ty, int* z0, int* nrows);
+
 /* One persistent launch over many grids of uneven sizes: `grids` (device)
  * holds `ngrids` descriptors from csd_grid_build, `item_start` (device) the
  * prefix sums of their work items (ngrids + 1 ints, last = total).  Work

@@ -225,6 +225,30 @@ def test_fused_boundary_step(kind, name):
         assert np.array_equal(t.cpu().numpy(), a)
 
 
+@pytest.mark.parametrize("kind", ["dirichlet", "neumann", "periodic", "reflecting"])
+@pytest.mark.parametrize("name,size", [("heat2d", (300, 700)), ("gs_u", (257, 1030)),
+                                       ("lap7", (26, 14, 522))])
+def test_fused_boundary_step_uneven_split(kind, name, size):
+    """Grids wide enough for the fused-boundary work split (shorter X-edge
+    items from the wave's spare slots, shorter first/last items)."""
+    import cutile
+
+    fn, ndim, nin = D.CASES[name]
+    bnd = {"type": kind, "value": -0.25} if kind == "dirichlet" else kind
+    r = cutile.compile(_stencil(fn, ndim, boundary=bnd), temporal_blocking=False)
+    shape = tuple(s + 2 * h for s, h in zip(size, r.halo_widths))
+    rng = np.random.default_rng(19)
+    ins = [rng.random(shape) for _ in range(nin)]
+    torch = _torch()
+    tin = [torch.from_numpy(a).cuda() for a in ins]
+    tout = torch.full_like(tin[0], float("nan"))
+    getattr(r.load_module(), f"step_{r.name}")(*tin, tout)
+    torch.cuda.synchronize()
+    want = O.stencil_with_boundary(ins, fn, ndim, r.halo_widths, kind, -0.25)
+    inner = _interior(shape, r.halo_widths)
+    assert np.array_equal(tout.cpu().numpy()[inner], want[inner])
+
+
 def test_compile_fused_gray_scott():
     import cutile
 

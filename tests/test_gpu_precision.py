@@ -17,13 +17,15 @@ def _fused(precision, boundary="periodic"):
                                 precision=precision, boundary=boundary)
 
 
-def test_kahan_step_bit_exact_against_numpy_float32():
+@pytest.mark.parametrize("n", [96, 700])
+def test_kahan_step_bit_exact_against_numpy_float32(n):
+    """n = 700 is wide enough for the fused-boundary work split."""
     import torch
 
     r = _fused("fp32_kahan")
     assert r.inputs == ("u", "v", "c_u", "c_v")
     h = r.halo_widths
-    u, v = D.gray_scott_init(96, seed=5, halo=h, dtype="float32")
+    u, v = D.gray_scott_init(n, seed=5, halo=h, dtype="float32")
     rng = np.random.default_rng(6)
     cu = (rng.standard_normal(u.shape) * 1e-8).astype(np.float32)
     cv = (rng.standard_normal(u.shape) * 1e-8).astype(np.float32)
