@@ -5,10 +5,12 @@ Replaces the reference's Dialect 3 -> cuTile Python emitter
 
 * the body becomes a device functor ``Body_<name>::compute``: for every
   distinct ``(field, z offset, y offset)`` it loads one row *strip* from the
-  staged tile (16-byte shared-memory vector loads), then evaluates each of
-  the thread's ``VEC`` points with one statement per SSA op of the DSL body,
-  in DSL order, using round-to-nearest intrinsics (``__dadd_rn`` ...) so no
-  multiply-add contraction or re-association can change a bit;
+  staged tile (16-byte shared-memory vector loads), then evaluates the
+  thread's ``VEC`` points with one statement per SSA op of the DSL body, in
+  DSL order, using round-to-nearest intrinsics (``__dadd_rn`` ...) so no
+  multiply-add contraction or re-association can change a bit; a value that
+  one point needs at an X shift of another point's value (a face flux, a
+  neighbour's velocity) is computed once (``_ShiftClasses``);
 * two kernels instantiate the engine template around it: ``<name>_tma``
   (TMA tile copies) and ``<name>_ldg`` (cp.async copies, for arrays whose
   row pitch is not 16-byte aligned);
@@ -157,6 +159,37 @@ class _BodyEmitter:
         return f"({store_t}){self.name(v)}"
 
 
+def _pos_name(cid: int, pos) -> str:
+    if pos is None:
+        return f"c{cid}"
+    return f"c{cid}_{'m' if pos < 0 else ''}{abs(pos)}"
+
+
+class _ShiftClasses:
+    """Values of the body up to a shift along X.
+
+    A value's class is its expression tree with every access's X offset made
+    relative to the smallest X offset in the tree (``mx``); the value at the
+    thread's point ``k`` is then its class at absolute position ``k + mx``.
+    Two values of one class at one position are the same expression of the
+    same staged cells, so a thread that evaluates ``VEC`` neighbouring points
+    computes each (class, position) once: a flux at the face between points k
+    and k+1 serves as the east flux of k and the west flux of k+1.  Every
+    value is still computed by the same round-to-nearest operations on the
+    same operands, so results are bit-identical to evaluating each point on
+    its own.
+    """
+
+    def __init__(self):
+        self.ids: dict = {}
+
+    def intern(self, key) -> int:
+        cid = self.ids.get(key)
+        if cid is None:
+            cid = self.ids[key] = len(self.ids)
+        return cid
+
+
 def emit_body(kernel: KernelOp) -> str:
     """Device functor for the kernel's stencil body(ies)."""
     name = kernel.kernel_name.data
@@ -164,6 +197,7 @@ def emit_body(kernel: KernelOp) -> str:
     dtype = kernel.dtype.data
     field_t = "f32" if dtype in ("float32", "fp32") else "f64"
     store_t = "float" if field_t == "f32" else "double"
+    vec = 4 if field_t == "f32" else 2   # 16 bytes of points per thread (engine Cfg::VEC)
     accesses = [tuple(a.data for a in acc) for acc in kernel.accesses.data]
     # group accesses by (field, dz, dy) -> x range
     groups: dict[tuple, list] = {}
@@ -178,7 +212,8 @@ def emit_body(kernel: KernelOp) -> str:
            "  template <class C>",
            "  __device__ __forceinline__ static void compute(const csd::TileView<C>& t, int r, int y,",
            "                                                 int x, csd::OutPack<typename C::T, "
-           "C::NOUT, C::VEC>& o) {"]
+           "C::NOUT, C::VEC>& o) {",
+           f"    static_assert(C::VEC == {vec}, \"body emitted for {vec} points per thread\");"]
     for gi, key in enumerate(gkeys):
         f, dz, dy = key
         lo, hi = min(groups[key]), max(groups[key])
@@ -192,21 +227,77 @@ def emit_body(kernel: KernelOp) -> str:
     for k in range(n_dyn):
         out.append(f"    const double d{k} = t.dynamic({k});")
         access_types[f"d{k}"] = "w"
-    out.append("#pragma unroll")
-    out.append("    for (int k = 0; k < C::VEC; ++k) {")
-    for j, (key, dx) in enumerate(acc_info):
-        gi = gkeys.index(key)
-        lo = min(groups[key])
-        out.append(f"      const {store_t} a{j} = st{gi}.v[k + {dx - lo}];")
-        access_types[f"a{j}"] = field_t
-    for m, prog in enumerate(kernel.ssa_body.data):
-        em = _BodyEmitter(f"p{m}_")
-        rets = em.emit([s.data for s in prog], access_types)
-        for line in em.lines:
-            out.append("      " + line)
-        for res, idx in rets:
-            out.append(f"      o.v[{m if idx is None else idx}][k] = {em.result_as(res, store_t)};")
-    out.append("    }")
+
+    # classes of every SSA value of every member (members share classes, so a
+    # value two fused members both compute is computed once too)
+    classes = _ShiftClasses()
+    members = []
+    for prog in kernel.ssa_body.data:
+        info: dict = {}        # SSA name -> (class id, mx or None)
+        lines, rets = [], []
+        for raw in (x.data for x in prog):
+            lhs, op, args, typ, extra = _parse_line(raw)
+            if op == "return":
+                rets.append((args[0], extra))
+                continue
+            if op == "const":
+                info[lhs] = (classes.intern(("const", typ, repr(extra))), None)
+                lines.append((lhs, op, [], typ, extra))
+                continue
+            parts = []
+            for a in args:
+                if a[0] == "a" and a[1:].isdigit():
+                    gkey, dx = acc_info[int(a[1:])]
+                    parts.append((classes.intern(("leaf", gkeys.index(gkey))), dx))
+                elif a[0] in "sd" and a[1:].isdigit():
+                    parts.append((classes.intern(("scalar", a)), None))
+                else:
+                    parts.append(info[a])
+            mxs = [m for _, m in parts if m is not None]
+            mx = min(mxs) if mxs else None
+            key = (op, typ, extra, tuple((c, None if m is None else m - mx) for c, m in parts))
+            info[lhs] = (classes.intern(key), mx)
+            lines.append((lhs, op, args, typ, extra))
+        members.append((info, lines, rets))
+
+    def rename(a: str, info: dict, k: int) -> str:
+        if a[0] == "a" and a[1:].isdigit():
+            gkey, dx = acc_info[int(a[1:])]
+            gi = gkeys.index(gkey)
+            leaf = f"L{gi}_{k + dx - min(groups[gkey])}"
+            if leaf not in access_types:
+                access_types[leaf] = field_t
+                out.append(f"    const {store_t} q_{leaf} = st{gi}.v[{k + dx - min(groups[gkey])}];")
+            return leaf
+        if a[0] in "sd" and a[1:].isdigit():
+            return a
+        cid, mx = info[a]
+        return _pos_name(cid, None if mx is None else k + mx)
+
+    emitted: set = set()
+    ssa: list[str] = []
+    stores = []
+    for k in range(vec):
+        for m, (info, lines, rets) in enumerate(members):
+            for lhs, op, args, typ, extra in lines:
+                nm = rename(lhs, info, k)
+                if nm in emitted:
+                    continue
+                emitted.add(nm)
+                if op == "const":
+                    ssa.append(f"{nm} = const {extra!r} : {typ}")
+                else:
+                    tail = f" @{extra}" if extra is not None else ""
+                    ssa.append(f"{nm} = {op} {', '.join(rename(a, info, k) for a in args)}{tail}"
+                               f" : {typ}")
+            for res, idx in rets:
+                stores.append((m if idx is None else idx, k, rename(res, info, k)))
+    em = _BodyEmitter("q_")
+    em.emit(ssa, access_types)
+    for line in em.lines:
+        out.append("    " + line)
+    for slot, k, res in stores:
+        out.append(f"    o.v[{slot}][{k}] = {em.result_as(res, store_t)};")
     out.append("  }")
     out.append("};")
     return "\n".join(out)

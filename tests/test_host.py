@@ -185,7 +185,29 @@ def test_emitted_kernel_keeps_term_order_and_exact_constants():
     assert "0x1.999999999999ap-4" in src
     assert "fma(" not in src
     adds = re.findall(r"__dadd_rn\((\w+), (\w+)\)", src)
-    assert adds[0] == ("a1", "a2")
+    # first addition: the z-1 and z+1 neighbours of point 0, in that order
+    assert adds[0] == ("q_L1_0", "q_L2_0")
+    assert "t.template strip<0, -1, 0, 0, 0>" in src.split("st1 =")[1].split(";")[0]
+    assert "q_L1_0 = st1.v[0];" in src and "q_L2_0 = st2.v[0];" in src
+
+
+def test_shifted_values_are_computed_once_per_position():
+    """A thread's neighbouring points share X-shifted subexpressions: the
+    shallow-water body's velocity hu/h and wave speed sqrt(g h) at the east,
+    centre and west cells of 4 points cover 6 positions, not 12."""
+    from cutile import compile as stencil_compile
+    from cutile import stencil
+
+    r = stencil_compile(stencil(ndim=2, dtype="float32")(D.sw_rhs), temporal_blocking=False,
+                        align_halo=False)
+    body = r.cuda_source.split("struct Body_")[1].split("};")[0]
+    sqrts = re.findall(r"csd::sqrt_rn\(", body)
+    # centre/east/west: positions -1..4 (6); north and south: 4 each
+    assert len(sqrts) == 6 + 4 + 4
+    # every output of every point is stored once
+    for f in range(3):
+        for k in range(4):
+            assert body.count(f"o.v[{f}][{k}] = ") == 1
 
 
 def test_generated_kernels_compile_with_nvrtc_without_spills():
