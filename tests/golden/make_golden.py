@@ -1,6 +1,7 @@
 """Generate golden fixtures by running the REFERENCE's own CPU executor.
 
-Run in a container that has the reference checkout (not on the GPU box):
+Run on a machine that has the reference checkout (the fixtures it writes are what
+the tests read; the tests never need the reference itself):
 
     python tests/golden/make_golden.py /path/to/reference
 
