@@ -355,3 +355,29 @@ def test_occupancy_hint_reaches_the_launch_bound():
     # without a hint the planner derives it from shared memory and registers
     r = stencil_compile(fn, temporal_blocking=False)
     assert "occupancy" not in r.kernel_hints
+
+
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+def test_body_emission_is_well_formed_on_random_expressions(tmp_path, dtype):
+    """The shift-shared body of every random expression defines each value
+    once, before its first use, and stores every output of every point once."""
+    import random_exprs
+
+    import cutile
+
+    vec = 2 if dtype == "float64" else 4
+    for seed in range(40):
+        ndim, nfields, radius, fields, idx, body = random_exprs.case(seed)
+        fn = random_exprs.build(tmp_path, f"e{seed}_{dtype}", fields, idx, body, dtype=dtype)
+        r = cutile.compile(fn, temporal_blocking=False, align_halo=bool(seed % 2))
+        text = r.cuda_source.split("struct Body_")[1].split("\n};")[0]
+        defined = set()
+        for line in text.splitlines():
+            m = re.match(r"\s*const (?:double|float|bool) (q_\w+) = (.*);$", line)
+            if m:
+                for used in re.findall(r"\bq_\w+", m.group(2)):
+                    assert used in defined, (seed, line)
+                assert m.group(1) not in defined, (seed, line)
+                defined.add(m.group(1))
+        for k in range(vec):
+            assert len(re.findall(rf"o\.v\[0\]\[{k}\] = ", text)) == 1, seed
