@@ -52,7 +52,7 @@ __host__ __device__ constexpr int imax(int a, int b) { return a > b ? a : b; }
 // ---------------------------------------------------------------------------
 template <typename T_, int NIN_, int NOUT_, int RZ_, int RY_, int RX_, int ROWS_, int TY_, int TX_,
           int NT_, int STAGES_, int TEMPORAL_, int LOADER_, int BC_, int REDUCE_ = 0,
-          int BRICK_ = 0>
+          int BRICK_ = 0, int RPY_ = 1>
 struct Cfg {
   typedef T_ T;
   // Bricked layout: BRICK_ = (ndim << 4) | log2(brick size), 0 = flat.
@@ -64,6 +64,9 @@ struct Cfg {
   static constexpr int NT = NT_, STAGES = STAGES_, TEMPORAL = TEMPORAL_;
   static constexpr int LOADER = LOADER_, BC = BC_;
   static constexpr int REDUCE = REDUCE_;  // 1: max-reduce output 0 into grid.red, store nothing
+  // Y rows per thread: a unit is RPY rows x VEC points, so the body can read
+  // the strip of row y + 1 at offset dy once for both rows that need it
+  static constexpr int RPY = RPY_;
   static constexpr int ALIGN = 16 / (int)sizeof(T);
   static constexpr int VEC = ALIGN;
   static constexpr int HC = RZ > 0 ? cdiv(RZ, ROWS) : 0;  // halo chunks per side, per step
@@ -106,6 +109,8 @@ struct Cfg {
   static_assert(TEMPORAL == 1 || (NIN == 1 && NOUT == 1), "temporal chains need one field");
   static_assert(HC * ROWS >= RZ, "halo chunks");
   static_assert(BC == CSD_BC_NONE || TEMPORAL == 1, "fused boundary fill is single-step");
+  static_assert(RPY >= 1 && TY % RPY == 0, "tile height must be a multiple of the rows per thread");
+  static_assert(RPY == 1 || TEMPORAL == 1, "temporal chains take one row per thread");
 };
 
 // ---------------------------------------------------------------------------
@@ -696,7 +701,8 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
           xv_hi = cdiv(C::PADL + C::TX + (T_ - s) * C::RX, C::VEC);
         }
         const int nxv = xv_hi - xv_lo;
-        const int units = C::ROWS * hs * nxv;
+        const int hsu = hs / C::RPY;  // units per chunk row along Y
+        const int units = C::ROWS * hsu * nxv;
         // Z row (interior index) of this chunk's first row for field s
         const int zrow0 = z0 + (k - HCT) * C::ROWS;
         const int ybuf0 = Y0 - (T_ - s) * C::RY;  // array row of dst buffer row 0
@@ -706,15 +712,20 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
         for (int u = threadIdx.x; u < units; u += C::NT) {
           const int xv = xv_lo + u % nxv;
           const int t2 = u / nxv;
-          const int y = t2 % hs;
-          const int r = t2 / hs;
-          OutPack<T, C::NOUT, C::VEC> o;
+          const int y = (t2 % hsu) * C::RPY;
+          const int r = t2 / hsu;
+          OutPack<T, C::NOUT, C::VEC * C::RPY> o;
           Body::template compute<C>(src, r, y, xv * C::VEC, o);
           const int gz = hz + zrow0 + r;                 // array coordinates
-          const int gy = ybuf0 + y;
           const int gx0 = X0 - C::PADL + xv * C::VEC;
           const bool zin = zrow0 + r >= 0 && zrow0 + r < nz;
+#pragma unroll
+          for (int j = 0; j < C::RPY; ++j) {
+          const int gy = ybuf0 + y + j;
           const bool yin = gy >= hy && gy < hy + ny;
+          const T* ov[C::NOUT];
+#pragma unroll
+          for (int f = 0; f < C::NOUT; ++f) ov[f] = o.v[f] + j * C::VEC;
           if (last) {
             if (!(zin && yin && (zrow0 + r) < z0 + nrows)) continue;
             if constexpr (C::REDUCE) {
@@ -722,7 +733,7 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
               for (int e = 0; e < C::VEC; ++e) {
                 const int gx = gx0 + e;
                 if (gx >= hx && gx < hx + nx) {
-                  const double v = (double)o.v[0][e];
+                  const double v = (double)ov[0][e];
                   red_acc = (v != v || v > red_acc) ? v : red_acc;
                 }
               }
@@ -735,12 +746,12 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
               for (int f = 0; f < C::NOUT; ++f) {
                 T* out = outp[f] + rowoff;
                 if (full && vec_store) {
-                  store_vec(out + gx0, o.v[f]);
+                  store_vec(out + gx0, ov[f]);
                 } else {
 #pragma unroll
                   for (int e = 0; e < C::VEC; ++e) {
                     const int gx = gx0 + e;
-                    if (gx >= hx && gx < hx + nx) out[gx] = o.v[f][e];
+                    if (gx >= hx && gx < hx + nx) out[gx] = ov[f][e];
                   }
                 }
               }
@@ -750,25 +761,26 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
 #pragma unroll
               for (int f = 0; f < C::NOUT; ++f) {
                 if (full && vec_store) {
-                  store_vec(outp[f] + off0, o.v[f]);
+                  store_vec(outp[f] + off0, ov[f]);
                 } else {
 #pragma unroll
                   for (int e = 0; e < C::VEC; ++e) {
                     const int gx = gx0 + e;
-                    if (gx >= hx && gx < hx + nx) outp[f][off0 + e] = o.v[f][e];
+                    if (gx >= hx && gx < hx + nx) outp[f][off0 + e] = ov[f][e];
                   }
                 }
               }
             }
           } else {
-            T* d = dst + (r * hs + y) * C::BOXW + xv * C::VEC;
+            T* d = dst + (r * hs + y + j) * C::BOXW + xv * C::VEC;
 #pragma unroll
             for (int e = 0; e < C::VEC; ++e) {
               const int gx = gx0 + e;
               const bool in = zin && yin && gx >= hx && gx < hx + nx;
-              d[e] = in ? o.v[0][e] : T(0);
+              d[e] = in ? ov[0][e] : T(0);
             }
           }
+          }  // rows of the unit
         }
         __syncthreads();
       }

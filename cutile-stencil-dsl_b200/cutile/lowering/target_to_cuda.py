@@ -162,22 +162,23 @@ class _BodyEmitter:
 def _pos_name(cid: int, pos) -> str:
     if pos is None:
         return f"c{cid}"
-    return f"c{cid}_{'m' if pos < 0 else ''}{abs(pos)}"
+    return "c%d_%s" % (cid, "_".join(("m%d" % -p) if p < 0 else str(p) for p in pos))
 
 
 class _ShiftClasses:
-    """Values of the body up to a shift along X.
+    """Values of the body up to a shift along Y and X.
 
-    A value's class is its expression tree with every access's X offset made
-    relative to the smallest X offset in the tree (``mx``); the value at the
-    thread's point ``k`` is then its class at absolute position ``k + mx``.
-    Two values of one class at one position are the same expression of the
-    same staged cells, so a thread that evaluates ``VEC`` neighbouring points
-    computes each (class, position) once: a flux at the face between points k
-    and k+1 serves as the east flux of k and the west flux of k+1.  Every
-    value is still computed by the same round-to-nearest operations on the
-    same operands, so results are bit-identical to evaluating each point on
-    its own.
+    A value's class is its expression tree with every access's Y and X
+    offsets made relative to the smallest Y and the smallest X offset in the
+    tree (``(my, mx)``); the value at the thread's point ``(j, k)`` (row j of
+    the unit, point k of the row) is then its class at absolute position
+    ``(j + my, k + mx)``.  Two values of one class at one position are the
+    same expression of the same staged cells, so a thread computes each
+    (class, position) once: a flux at the face between points k and k+1
+    serves as the east flux of k and the west flux of k+1, and a strip of
+    row y + 1 read at offset dy serves row y at offset dy + 1.  Every value is
+    still computed by the same round-to-nearest operations on the same
+    operands, so results are bit-identical to evaluating each point alone.
     """
 
     def __init__(self):
@@ -198,22 +199,23 @@ def emit_body(kernel: KernelOp) -> str:
     field_t = "f32" if dtype in ("float32", "fp32") else "f64"
     store_t = "float" if field_t == "f32" else "double"
     vec = 4 if field_t == "f32" else 2   # 16 bytes of points per thread (engine Cfg::VEC)
+    rpy = engine_params(kernel)["RPY"]   # Y rows per thread (engine Cfg::RPY)
     accesses = [tuple(a.data for a in acc) for acc in kernel.accesses.data]
-    # group accesses by (field, dz, dy) -> x range
+    acc_info = [_internal_offsets(ndim, offs) + (f,) for f, *offs in accesses]  # (dz, dy, dx, f)
+    # strip groups: (field, dz, dy of the unit's row 0) -> X range, over all rows
     groups: dict[tuple, list] = {}
-    acc_info = []
-    for j, (f, *offs) in enumerate(accesses):
-        dz, dy, dx = _internal_offsets(ndim, offs)
-        key = (f, dz, dy)
-        groups.setdefault(key, []).append(dx)
-        acc_info.append((key, dx))
+    for dz, dy, dx, f in acc_info:
+        for j in range(rpy):
+            groups.setdefault((f, dz, dy + j), []).append(dx)
     gkeys = list(groups)
+    gindex = {key: gi for gi, key in enumerate(gkeys)}
     out = [f"struct Body_{name} {{",
            "  template <class C>",
            "  __device__ __forceinline__ static void compute(const csd::TileView<C>& t, int r, int y,",
            "                                                 int x, csd::OutPack<typename C::T, "
-           "C::NOUT, C::VEC>& o) {",
-           f"    static_assert(C::VEC == {vec}, \"body emitted for {vec} points per thread\");"]
+           "C::NOUT, C::VEC * C::RPY>& o) {",
+           f"    static_assert(C::VEC == {vec} && C::RPY == {rpy}, "
+           f"\"body emitted for {vec} points x {rpy} rows per thread\");"]
     for gi, key in enumerate(gkeys):
         f, dz, dy = key
         lo, hi = min(groups[key]), max(groups[key])
@@ -233,7 +235,7 @@ def emit_body(kernel: KernelOp) -> str:
     classes = _ShiftClasses()
     members = []
     for prog in kernel.ssa_body.data:
-        info: dict = {}        # SSA name -> (class id, mx or None)
+        info: dict = {}        # SSA name -> (class id, (my, mx) or None)
         lines, rets = [], []
         for raw in (x.data for x in prog):
             lhs, op, args, typ, extra = _parse_line(raw)
@@ -247,57 +249,61 @@ def emit_body(kernel: KernelOp) -> str:
             parts = []
             for a in args:
                 if a[0] == "a" and a[1:].isdigit():
-                    gkey, dx = acc_info[int(a[1:])]
-                    parts.append((classes.intern(("leaf", gkeys.index(gkey))), dx))
+                    dz, dy, dx, f = acc_info[int(a[1:])]
+                    parts.append((classes.intern(("leaf", f, dz)), (dy, dx)))
                 elif a[0] in "sd" and a[1:].isdigit():
                     parts.append((classes.intern(("scalar", a)), None))
                 else:
                     parts.append(info[a])
-            mxs = [m for _, m in parts if m is not None]
-            mx = min(mxs) if mxs else None
-            key = (op, typ, extra, tuple((c, None if m is None else m - mx) for c, m in parts))
-            info[lhs] = (classes.intern(key), mx)
+            pos = [m for _, m in parts if m is not None]
+            mn = (min(m[0] for m in pos), min(m[1] for m in pos)) if pos else None
+            key = (op, typ, extra, tuple(
+                (c, None if m is None else (m[0] - mn[0], m[1] - mn[1])) for c, m in parts))
+            info[lhs] = (classes.intern(key), mn)
             lines.append((lhs, op, args, typ, extra))
         members.append((info, lines, rets))
 
-    def rename(a: str, info: dict, k: int) -> str:
+    def rename(a: str, info: dict, j: int, k: int) -> str:
         if a[0] == "a" and a[1:].isdigit():
-            gkey, dx = acc_info[int(a[1:])]
-            gi = gkeys.index(gkey)
-            leaf = f"L{gi}_{k + dx - min(groups[gkey])}"
+            dz, dy, dx, f = acc_info[int(a[1:])]
+            key = (f, dz, dy + j)
+            gi = gindex[key]
+            idx = k + dx - min(groups[key])
+            leaf = f"L{gi}_{idx}"
             if leaf not in access_types:
                 access_types[leaf] = field_t
-                out.append(f"    const {store_t} q_{leaf} = st{gi}.v[{k + dx - min(groups[gkey])}];")
+                out.append(f"    const {store_t} q_{leaf} = st{gi}.v[{idx}];")
             return leaf
         if a[0] in "sd" and a[1:].isdigit():
             return a
-        cid, mx = info[a]
-        return _pos_name(cid, None if mx is None else k + mx)
+        cid, mn = info[a]
+        return _pos_name(cid, None if mn is None else (j + mn[0], k + mn[1]))
 
     emitted: set = set()
     ssa: list[str] = []
     stores = []
-    for k in range(vec):
-        for m, (info, lines, rets) in enumerate(members):
-            for lhs, op, args, typ, extra in lines:
-                nm = rename(lhs, info, k)
-                if nm in emitted:
-                    continue
-                emitted.add(nm)
-                if op == "const":
-                    ssa.append(f"{nm} = const {extra!r} : {typ}")
-                else:
-                    tail = f" @{extra}" if extra is not None else ""
-                    ssa.append(f"{nm} = {op} {', '.join(rename(a, info, k) for a in args)}{tail}"
-                               f" : {typ}")
-            for res, idx in rets:
-                stores.append((m if idx is None else idx, k, rename(res, info, k)))
+    for j in range(rpy):
+        for k in range(vec):
+            for m, (info, lines, rets) in enumerate(members):
+                for lhs, op, args, typ, extra in lines:
+                    nm = rename(lhs, info, j, k)
+                    if nm in emitted:
+                        continue
+                    emitted.add(nm)
+                    if op == "const":
+                        ssa.append(f"{nm} = const {extra!r} : {typ}")
+                    else:
+                        tail = f" @{extra}" if extra is not None else ""
+                        ssa.append(f"{nm} = {op} {', '.join(rename(a, info, j, k) for a in args)}"
+                                   f"{tail} : {typ}")
+                for res, idx in rets:
+                    stores.append((m if idx is None else idx, j * vec + k, rename(res, info, j, k)))
     em = _BodyEmitter("q_")
     em.emit(ssa, access_types)
     for line in em.lines:
         out.append("    " + line)
-    for slot, k, res in stores:
-        out.append(f"    o.v[{slot}][{k}] = {em.result_as(res, store_t)};")
+    for slot, e, res in stores:
+        out.append(f"    o.v[{slot}][{e}] = {em.result_as(res, store_t)};")
     out.append("  }")
     out.append("};")
     return "\n".join(out)
@@ -347,6 +353,7 @@ def engine_params(kernel: KernelOp) -> dict:
         "NDYN": kernel.dyn_count.data if kernel.dyn_count is not None else 0,
         "REDUCE": kernel.reduce_max.data if kernel.reduce_max is not None else 0,
         "BRICK": _brick_code(kernel, ndim),
+        "RPY": int(hints.get("rpy", 1)),
     }
 
 
@@ -389,7 +396,7 @@ def emit_cuda(module: ModuleOp, preamble: bool = True) -> str:
                 loader = "CSD_LOADER_LDG"   # bricked fields: both entries use cp.async
             cfg = (f"csd::Cfg<{p['T']}, {p['NIN']}, {p['NOUT']}, {p['RZ']}, {p['RY']}, {p['RX']}, "
                    f"{p['ROWS']}, {p['TY']}, {p['TX']}, {p['NT']}, {p['STAGES']}, {p['TEMPORAL']}, "
-                   f"{loader}, {p['BC']}, {p['REDUCE']}, {p['BRICK']}>")
+                   f"{loader}, {p['BC']}, {p['REDUCE']}, {p['BRICK']}, {p['RPY']}>")
             parts.append(f"typedef {cfg} Cfg_{name}_{suffix};")
             parts.append(f'extern "C" __global__ void __launch_bounds__({p["NT"]}, {p["MINB"]})')
             parts.append(f"{name}_{suffix}(const __grid_constant__ csd_params p) {{")

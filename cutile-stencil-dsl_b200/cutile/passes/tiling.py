@@ -152,10 +152,11 @@ class EnginePlan:
     min_blocks: int = 1        # resident blocks per SM the launch bound asks for (fit_plan)
     occupancy: int = 0         # explicit min_blocks request (0: fit_plan chooses)
     waves: int = 0             # auto zchunk: work items per resident block (0: fit_plan chooses)
+    rpy: int = 1               # Y rows per thread (3-D, single step): strips shared by rows
 
     @property
     def units_per_step(self) -> int:
-        return self.rows * self.tile_y * (self.tile_x // self.vec)
+        return self.rows * (self.tile_y // self.rpy) * (self.tile_x // self.vec)
 
     @property
     def units_per_thread(self) -> int:
@@ -169,8 +170,11 @@ class EnginePlan:
         return (self.tile_x,)
 
     def hints(self) -> dict:
-        return {"threads": self.threads, "vec": self.vec, "stages": self.stages,
-                "zchunk": self.zchunk, "min_blocks": self.min_blocks, "waves": self.waves}
+        h = {"threads": self.threads, "vec": self.vec, "stages": self.stages,
+             "zchunk": self.zchunk, "min_blocks": self.min_blocks, "waves": self.waves}
+        if self.rpy != 1:
+            h["rpy"] = self.rpy
+        return h
 
 
 def _align_up(x: int, a: int) -> int:
@@ -262,6 +266,8 @@ def fit_plan(plan: EnginePlan, radius: tuple[int, ...], dtype_bytes: int,
              num_inputs: int, body_ops: int = 0, periodic: bool = False) -> EnginePlan:
     """Shrink a plan until its TMA box and shared memory fit the B200 limits."""
     r3 = radius3(plan.ndim, radius)
+    if plan.rpy != 1 and (plan.ndim != 3 or plan.temporal != 1 or plan.rpy < 1):
+        raise ValueError("rows per thread > 1 needs a 3-D single-step stencil")
     for _ in range(64):
         g = engine_geometry(plan, r3, dtype_bytes, num_inputs, periodic)
         ok_box = g["box_w"] <= TMA_BOX_MAX and g["box_h"] <= TMA_BOX_MAX
@@ -271,12 +277,14 @@ def fit_plan(plan: EnginePlan, radius: tuple[int, ...], dtype_bytes: int,
             plan = replace(plan, stages=plan.stages - 1)
         elif plan.tile_x > 32 and (not ok_box or plan.tile_x >= plan.tile_y * 8):
             plan = replace(plan, tile_x=plan.tile_x // 2)
-        elif plan.tile_y > 1:
-            plan = replace(plan, tile_y=plan.tile_y // 2)
+        elif plan.tile_y > plan.rpy:
+            plan = replace(plan, tile_y=max(plan.rpy, plan.tile_y // 2))
         elif plan.rows > 1 and plan.rows // 2 >= 1:
             plan = replace(plan, rows=plan.rows // 2)
         else:
             raise ValueError(f"stencil footprint {radius} does not fit the B200 engine")
+    if plan.tile_y % plan.rpy:
+        raise ValueError(f"tile height {plan.tile_y} is not a multiple of {plan.rpy} rows per thread")
     units = plan.units_per_step
     threads = min(plan.threads, units)
     while units % threads:
@@ -287,7 +295,7 @@ def fit_plan(plan: EnginePlan, radius: tuple[int, ...], dtype_bytes: int,
     # resident blocks the shared memory allows, capped so the register budget
     # stays >= 64 per thread (128 for long bodies such as flux stencils, which
     # otherwise spill); the launch bound is a hint to ptxas, not a floor
-    regs = 128 if body_ops > 120 else 64
+    regs = 128 if body_ops > 120 or plan.rpy > 1 else 64
     fit_blocks = max(1, min(B200_SMEM_PER_SM // max(1, g["smem_bytes"] + 1024),
                             B200_MAX_THREADS_PER_SM // threads))
     if plan.occupancy > 0:    # an explicit occupancy hint, capped by what fits

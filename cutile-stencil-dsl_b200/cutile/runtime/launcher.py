@@ -335,6 +335,8 @@ def _plan_from(tile_sizes, kernel_hints, ndim, base_plan):
         for k in ("threads", "stages", "zchunk", "waves"):
             if k in kernel_hints:
                 kw[k] = int(kernel_hints[k])
+        if "rows_per_thread" in kernel_hints:
+            kw["rpy"] = int(kernel_hints["rows_per_thread"])
         occ = kernel_hints.get("min_blocks", kernel_hints.get("occupancy"))
         if occ is not None:
             kw["occupancy"] = int(occ)
