@@ -237,6 +237,15 @@ def default_engine_plan(ndim: int, num_loads: int, dtype_bytes: int, radius: tup
                               zchunk=0)
         if wide:
             plan = replace(plan, tile_y=4, tile_x=64)
+            if dtype_bytes == 8 and num_inputs == 1 and num_outputs == 1:
+                # measured on B200 (dense boxes, 512^3 FP64): a thread owning
+                # several Y rows reads each staged strip once for all of them;
+                # 27 points: 4 rows over 16x64, 136 -> 264 GPts/s; 125 points
+                # (radius 2, more strips live): 2 rows over 2x4x128, 55 -> 87
+                if max(radius[1], radius[2]) <= 1:
+                    plan = replace(plan, rows=1, tile_y=16, tile_x=64, threads=128, rpy=4)
+                else:
+                    plan = replace(plan, rows=2, tile_y=4, tile_x=128, threads=128, rpy=2)
     elif ndim == 2:
         # short single-field bodies (5/9-point) run best with 128 threads per
         # 8x128 tile (autotuned, heat 4096^2: FP32 27 vs 32 us per step);
@@ -330,6 +339,8 @@ class EngineTilingPass(ModulePass):
                 plan = default_engine_plan(len(halo), unique_access_count(child), self.dtype_bytes,
                                            halo, nin)
                 if self.overrides or self.temporal_steps != 1:
+                    if self.temporal_steps != 1:
+                        plan = replace(plan, rpy=1)   # temporal chains: one row per thread
                     plan = fit_plan(replace(plan, temporal=self.temporal_steps, **self.overrides),
                                     halo, self.dtype_bytes, nin)
                 child.attributes["engine_tile"] = ArrayAttr([IntAttr(t) for t in plan.tile_sizes()])

@@ -323,6 +323,8 @@ def _plan_from(tile_sizes, kernel_hints, ndim, base_plan):
 
     p = base_plan
     if tile_sizes is not None:
+        # a caller's tile keeps one row per thread unless it asks for more
+        p = replace(p, rpy=1)
         t = tuple(tile_sizes)
         if ndim == 3:
             p = replace(p, rows=t[0], tile_y=t[1], tile_x=t[2])
@@ -530,7 +532,8 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
         # (stencil_to_target.py:796-800), so a multi-field stencil cannot run
         # blocked there either; it advances one step per launch.
         T = 1
-    plan = _plan_from(tile_sizes, kernel_hints, len(stencil_halo), replace(plan, temporal=T))
+    plan = _plan_from(tile_sizes, kernel_hints, len(stencil_halo),
+                      replace(plan, temporal=T, rpy=plan.rpy if T == 1 else 1))
     if occupancy is not None:
         plan = replace(plan, occupancy=int(occupancy))
     plan = fit_plan(plan, stencil_halo, dtype_bytes, num_inputs, analysis.get("body_ops", 0))

@@ -381,3 +381,33 @@ def test_body_emission_is_well_formed_on_random_expressions(tmp_path, dtype):
                 defined.add(m.group(1))
         for k in range(vec):
             assert len(re.findall(rf"o\.v\[0\]\[{k}\] = ", text)) == 1, seed
+
+
+def test_rows_per_thread_plans():
+    """Dense FP64 boxes default to several Y rows per thread (measured
+    faster); temporal chains, caller tiles and other stencils keep one."""
+    import wide_defs as W
+
+    from dataclasses import replace
+
+    from cutile import compile as stencil_compile
+    from cutile import stencil
+    from cutile.passes.tiling import EnginePlan, fit_plan
+
+    r27 = stencil_compile(W.load_box("box27_plan", 1), temporal_blocking=False)
+    assert r27.tile_sizes == (1, 16, 64) and r27.kernel_hints["rpy"] == 4
+    assert ", 4> Cfg_box27_plan_tma;" in r27.cuda_source
+    r125 = stencil_compile(W.load_box("box125_plan", 2), temporal_blocking=False)
+    assert r125.tile_sizes == (2, 4, 128) and r125.kernel_hints["rpy"] == 2
+    assert "rpy" not in stencil_compile(W.load_box("box27_plan", 1)).kernel_hints  # T = 2
+    assert "rpy" not in stencil_compile(W.load_box("box27_plan", 1), temporal_blocking=False,
+                                        tile_sizes=(1, 4, 64)).kernel_hints
+    assert "rpy" not in stencil_compile(W.load_box("box27_f32", 1, dtype="float32"),
+                                        temporal_blocking=False).kernel_hints
+    assert "rpy" not in stencil_compile(stencil(ndim=3)(D.lap7), temporal_blocking=False).kernel_hints
+    p = EnginePlan(3, rows=1, tile_y=8, tile_x=64, vec=2, threads=128, stages=1, zchunk=0, rpy=2)
+    assert fit_plan(p, (1, 1, 1), 8, 1).units_per_step == 8 // 2 * 32
+    with pytest.raises(ValueError):
+        fit_plan(replace(p, temporal=2), (1, 1, 1), 8, 1)
+    with pytest.raises(ValueError):
+        fit_plan(replace(p, tile_y=6, rpy=4), (1, 1, 1), 8, 1)
