@@ -721,65 +721,65 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
           const bool zin = zrow0 + r >= 0 && zrow0 + r < nz;
 #pragma unroll
           for (int j = 0; j < C::RPY; ++j) {
-          const int gy = ybuf0 + y + j;
-          const bool yin = gy >= hy && gy < hy + ny;
-          const T* ov[C::NOUT];
+            const int gy = ybuf0 + y + j;
+            const bool yin = gy >= hy && gy < hy + ny;
+            const T* ov[C::NOUT];
 #pragma unroll
-          for (int f = 0; f < C::NOUT; ++f) ov[f] = o.v[f] + j * C::VEC;
-          if (last) {
-            if (!(zin && yin && (zrow0 + r) < z0 + nrows)) continue;
-            if constexpr (C::REDUCE) {
+            for (int f = 0; f < C::NOUT; ++f) ov[f] = o.v[f] + j * C::VEC;
+            if (last) {
+              if (!(zin && yin && (zrow0 + r) < z0 + nrows)) continue;
+              if constexpr (C::REDUCE) {
 #pragma unroll
-              for (int e = 0; e < C::VEC; ++e) {
-                const int gx = gx0 + e;
-                if (gx >= hx && gx < hx + nx) {
-                  const double v = (double)ov[0][e];
-                  red_acc = (v != v || v > red_acc) ? v : red_acc;
+                for (int e = 0; e < C::VEC; ++e) {
+                  const int gx = gx0 + e;
+                  if (gx >= hx && gx < hx + nx) {
+                    const double v = (double)ov[0][e];
+                    red_acc = (v != v || v > red_acc) ? v : red_acc;
+                  }
                 }
+                continue;
               }
-              continue;
-            }
-            const bool full = gx0 >= hx && gx0 + C::VEC <= hx + nx;
-            if constexpr (C::BRICK_SHIFT == 0) {
-              const long long rowoff = (long long)gz * pitch_z + (long long)gy * pitch_y;
+              const bool full = gx0 >= hx && gx0 + C::VEC <= hx + nx;
+              if constexpr (C::BRICK_SHIFT == 0) {
+                const long long rowoff = (long long)gz * pitch_z + (long long)gy * pitch_y;
 #pragma unroll
-              for (int f = 0; f < C::NOUT; ++f) {
-                T* out = outp[f] + rowoff;
-                if (full && vec_store) {
-                  store_vec(out + gx0, ov[f]);
-                } else {
+                for (int f = 0; f < C::NOUT; ++f) {
+                  T* out = outp[f] + rowoff;
+                  if (full && vec_store) {
+                    store_vec(out + gx0, ov[f]);
+                  } else {
 #pragma unroll
-                  for (int e = 0; e < C::VEC; ++e) {
-                    const int gx = gx0 + e;
-                    if (gx >= hx && gx < hx + nx) out[gx] = ov[f][e];
+                    for (int e = 0; e < C::VEC; ++e) {
+                      const int gx = gx0 + e;
+                      if (gx >= hx && gx < hx + nx) out[gx] = ov[f][e];
+                    }
+                  }
+                }
+              } else {
+                // a VEC-aligned run of VEC points stays inside one brick row
+                const long long off0 = elem_off<C>(g, gz, gy, gx0);
+#pragma unroll
+                for (int f = 0; f < C::NOUT; ++f) {
+                  if (full && vec_store) {
+                    store_vec(outp[f] + off0, ov[f]);
+                  } else {
+#pragma unroll
+                    for (int e = 0; e < C::VEC; ++e) {
+                      const int gx = gx0 + e;
+                      if (gx >= hx && gx < hx + nx) outp[f][off0 + e] = ov[f][e];
+                    }
                   }
                 }
               }
             } else {
-              // a VEC-aligned run of VEC points stays inside one brick row
-              const long long off0 = elem_off<C>(g, gz, gy, gx0);
+              T* d = dst + (r * hs + y + j) * C::BOXW + xv * C::VEC;
 #pragma unroll
-              for (int f = 0; f < C::NOUT; ++f) {
-                if (full && vec_store) {
-                  store_vec(outp[f] + off0, ov[f]);
-                } else {
-#pragma unroll
-                  for (int e = 0; e < C::VEC; ++e) {
-                    const int gx = gx0 + e;
-                    if (gx >= hx && gx < hx + nx) outp[f][off0 + e] = ov[f][e];
-                  }
-                }
+              for (int e = 0; e < C::VEC; ++e) {
+                const int gx = gx0 + e;
+                const bool in = zin && yin && gx >= hx && gx < hx + nx;
+                d[e] = in ? ov[0][e] : T(0);
               }
             }
-          } else {
-            T* d = dst + (r * hs + y + j) * C::BOXW + xv * C::VEC;
-#pragma unroll
-            for (int e = 0; e < C::VEC; ++e) {
-              const int gx = gx0 + e;
-              const bool in = zin && yin && gx >= hx && gx < hx + nx;
-              d[e] = in ? ov[0][e] : T(0);
-            }
-          }
           }  // rows of the unit
         }
         __syncthreads();
