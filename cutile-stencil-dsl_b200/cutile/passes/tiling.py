@@ -237,12 +237,14 @@ def default_engine_plan(ndim: int, num_loads: int, dtype_bytes: int, radius: tup
                               zchunk=0)
         if wide:
             plan = replace(plan, tile_y=4, tile_x=64)
-            if dtype_bytes == 8 and num_inputs == 1 and num_outputs == 1:
+            if (dtype_bytes == 8 and num_inputs == 1 and num_outputs == 1
+                    and max(radius) <= 2):
                 # measured on B200 (dense boxes, 512^3 FP64): a thread owning
                 # several Y rows reads each staged strip once for all of them;
                 # 27 points: 4 rows over 16x64, 136 -> 264 GPts/s; 125 points
-                # (radius 2, more strips live): 2 rows over 2x4x128, 55 -> 87
-                if max(radius[1], radius[2]) <= 1:
+                # (radius 2, more strips live): 2 rows over 2x4x128, 55 -> 87.
+                # Wider footprints keep one row (their strips would spill).
+                if max(radius) <= 1:
                     plan = replace(plan, rows=1, tile_y=16, tile_x=64, threads=128, rpy=4)
                 else:
                     plan = replace(plan, rows=2, tile_y=4, tile_x=128, threads=128, rpy=2)
