@@ -11,6 +11,7 @@
 #include "../../include/csd.h"
 
 extern "C" int csd_internal_fail(int code, const char* msg);
+extern "C" unsigned long long csd_internal_ctx_id(void);
 
 namespace {
 
@@ -422,9 +423,12 @@ namespace {
 static __device__ __align__(256) double g_noalloc_partials[CSD_NOALLOC_MAX_BLOCKS];
 
 // Device address of g_noalloc_partials per device ordinal (the host-side
-// name is only a stand-in for the symbol, never a device pointer).
+// name is only a stand-in for the symbol, never a device pointer), with the id
+// of the context it was looked up in: after cudaDeviceReset the device gets a
+// new context, the old address is void, and the next call looks it up again.
 std::mutex g_noalloc_mu;
 double* g_noalloc_ptr[64] = {nullptr};
+unsigned long long g_noalloc_ctx[64] = {0};
 
 int noalloc_scratch(double** out) {
   int dev = 0;
@@ -432,12 +436,14 @@ int noalloc_scratch(double** out) {
   if (e != cudaSuccess) return csd_internal_fail(CSD_ENODEV, cudaGetErrorString(e));
   if (dev < 0 || dev >= 64) return csd_internal_fail(CSD_EINVAL, "device ordinal out of range");
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
+  const unsigned long long ctx = csd_internal_ctx_id();
+  if (!g_noalloc_ptr[dev] || ctx == 0 || ctx != g_noalloc_ctx[dev]) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_partials);
     if (e != cudaSuccess)
       return csd_internal_fail(CSD_ELAUNCH, cudaGetErrorString(e));
     g_noalloc_ptr[dev] = static_cast<double*>(p);
+    g_noalloc_ctx[dev] = csd_internal_ctx_id();  // the lookup may have created the context
   }
   *out = g_noalloc_ptr[dev];
   return CSD_OK;

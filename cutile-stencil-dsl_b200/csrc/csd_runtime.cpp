@@ -76,6 +76,7 @@ struct Driver {
                                      int, int, int, int);
   CUresult (*cuGetErrorString)(CUresult, const char**);
   CUresult (*cuCtxSynchronize)(void);
+  CUresult (*cuCtxGetId)(CUcontext, unsigned long long*);  // optional (driver >= 12.0)
 };
 
 static thread_local std::string g_last_error;
@@ -135,6 +136,7 @@ static void load_driver(Driver& d) {
   CSD_SYM(cuGetErrorString, "cuGetErrorString");
   CSD_SYM(cuCtxSynchronize, "cuCtxSynchronize");
 #undef CSD_SYM
+  d.cuCtxGetId = reinterpret_cast<decltype(d.cuCtxGetId)>(dlsym(h, "cuCtxGetId"));
   if (d.cuInit(0) != 0) {
     d.why = "cuInit failed (no usable device)";
     return;
@@ -233,6 +235,18 @@ static bool read_file(const std::string& path, std::string* out) {
   return true;
 }
 
+// An ELF image (the only thing NVRTC's cubin output can be).
+static bool cubin_ok(const std::string& b) {
+  return b.size() >= 64 && (unsigned char)b[0] == 0x7f && b[1] == 'E' && b[2] == 'L' && b[3] == 'F';
+}
+
+// Integrity record of a cached cubin: its size and FNV-1a hash.
+static std::string cubin_sum(const std::string& b) {
+  char s[64];
+  snprintf(s, sizeof(s), "%zu %016llx\n", b.size(), fnv1a(b));
+  return s;
+}
+
 static int jit_compile(const char* src, int n_headers, const char* const* headers,
                        const char* const* header_names, const char* options, const char* cache_dir,
                        std::string* cubin, std::string* path_out, std::string* log_out) {
@@ -251,16 +265,23 @@ static int jit_compile(const char* src, int n_headers, const char* const* header
   key += "\n//nvrtc:" + std::to_string(major) + "." + std::to_string(minor);
   char hex[32];
   snprintf(hex, sizeof(hex), "%016llx", fnv1a(key));
-  std::string path;
+  std::string path, sumpath;
   if (cache_dir && *cache_dir) {
     mkdir(cache_dir, 0755);
     path = std::string(cache_dir) + "/" + hex + ".cubin";
+    sumpath = std::string(cache_dir) + "/" + hex + ".sum";
     std::string logpath = std::string(cache_dir) + "/" + hex + ".log";
-    if (read_file(path, cubin) && !cubin->empty()) {
+    std::string sum;
+    // A cache entry is used only when it is an ELF image whose size and
+    // checksum match the record written with it; a truncated, overwritten or
+    // half-written entry is compiled again and replaced.
+    if (read_file(path, cubin) && read_file(sumpath, &sum) && cubin_ok(*cubin) &&
+        sum == cubin_sum(*cubin)) {
       if (path_out) *path_out = path;
       if (log_out) read_file(logpath, log_out);
       return CSD_OK;
     }
+    cubin->clear();
   }
   nvrtcProgram prog;
   nvrtcResult rr = nvrtcCreateProgram(&prog, src, "stencil.cu", n_headers, headers, header_names);
@@ -296,6 +317,14 @@ static int jit_compile(const char* src, int n_headers, const char* const* header
       f.write(cubin->data(), (std::streamsize)cubin->size());
     }
     rename(tmp.c_str(), path.c_str());
+    {
+      std::string stmp = sumpath + ".tmp" + std::to_string(getpid());
+      {
+        std::ofstream f(stmp, std::ios::binary);
+        f << cubin_sum(*cubin);
+      }
+      rename(stmp.c_str(), sumpath.c_str());
+    }
     std::ofstream lf(std::string(cache_dir) + "/" + hex + ".log");
     lf << log;
     if (path_out) *path_out = path;
@@ -322,6 +351,18 @@ struct csd_kernel {
 extern "C" {
 
 int csd_internal_fail(int code, const char* msg) { return fail(code, "%s", msg); }
+
+// Unique id of the calling thread's current CUDA context (0: none current, or
+// the driver cannot say).  Lets callers notice that a device's context was
+// destroyed and re-created (cudaDeviceReset) since they cached an address.
+unsigned long long csd_internal_ctx_id(void) {
+  Driver& d = drv();
+  if (!d.ok || !d.cuCtxGetId) return 0;
+  CUcontext c = nullptr;
+  if (d.cuCtxGetCurrent(&c) != 0 || !c) return 0;
+  unsigned long long id = 0;
+  return d.cuCtxGetId(c, &id) == 0 ? id : 0;
+}
 
 int csd_version(void) { return 101; }
 
@@ -730,6 +771,7 @@ int csd_launch(csd_kernel* k, const csd_field* in, int n_in, const csd_field* ou
   if (rc) return rc;
   p.err = reinterpret_cast<int*>(st->err);
   p.timeout_ns = o.timeout_ns ? o.timeout_ns : 2000000000ull;
+  p.withhold = o.withhold_chunk > 0 ? o.withhold_chunk : 0;
   int grid = o.grid > 0 ? o.grid : k->blocks_per_sm[loader] * st->sms;
   if (grid > p.g.items) grid = p.g.items;
   if (grid < 1) return CSD_OK;  // nothing to do
@@ -782,6 +824,7 @@ int csd_launch_batch(csd_kernel* k, const csd_grid* grids, const int* item_start
   p.total_items = total_items;
   p.err = reinterpret_cast<int*>(st->err);
   p.timeout_ns = (opts && opts->timeout_ns) ? opts->timeout_ns : 2000000000ull;
+  p.withhold = (opts && opts->withhold_chunk > 0) ? opts->withhold_chunk : 0;
   const int loader = (opts && opts->loader == CSD_LOADER_LDG) ? CSD_LOADER_LDG : CSD_LOADER_TMA;
   int grid = (opts && opts->grid > 0) ? opts->grid : k->blocks_per_sm[loader] * st->sms;
   if (grid > total_items) grid = total_items;
@@ -812,6 +855,9 @@ int csd_error_word(int* value, int reset) {
     r = d.cuMemcpyHtoD(st->err, &zero, sizeof(int));
     if (r) return cu_fail(r, "cuMemcpyHtoD(error word)");
   }
+  if (v == CSD_ERR_TIMEOUT)
+    return fail(CSD_ETIMEOUT, "a kernel gave up waiting for its input (device error word 0x%x)", v);
+  if (v) return fail(CSD_ELAUNCH, "device error word 0x%x", v);
   return CSD_OK;
 }
 

@@ -28,6 +28,9 @@
 
 namespace csd {
 
+// Bound on the drain of an aborted work item (copies still in flight).
+constexpr unsigned long long kDrainNs = 2000000000ull;
+
 template <typename T>
 struct VecOf;
 template <>
@@ -630,6 +633,10 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
 #pragma unroll
     for (int f = 0; f < C::NOUT; ++f) outp[f] = reinterpret_cast<T*>(g.out[f]);
 
+    // failure-test hook: the first item of CTA 0 never requests input chunk
+    // `hold`, so the wait for it runs out (csd_launch_opts::withhold_chunk)
+    const int hold = (p.withhold > 0 && blockIdx.x == 0 && gitem == (int)blockIdx.x) ? p.withhold - 1 : -1;
+
     // prologue: fill the ring
     const int pre = min(nchunks, C::NSLOT);
     int issued = pre;   // chunks [0, issued) have been issued
@@ -637,7 +644,8 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
     for (int k = 0; k < pre; ++k) {
       const unsigned gq = seq + k;
       const int slot = gq % C::NSLOT;
-      Loader<C>::issue(g, ring, ptx::smem_addr(&bars[slot]), slot, cx, cy, cz + k * C::ROWS);
+      if (k != hold)
+        Loader<C>::issue(g, ring, ptx::smem_addr(&bars[slot]), slot, cx, cy, cz + k * C::ROWS);
     }
 
     for (int i = 0; i < nchunks; ++i) {
@@ -793,17 +801,23 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
           const unsigned gq = seq + nk;
           const int slot = gq % C::NSLOT;
           if (C::LOADER == CSD_LOADER_TMA && threadIdx.x == 0) ptx::fence_proxy_async_smem();
-          Loader<C>::issue(g, ring, ptx::smem_addr(&bars[slot]), slot, cx, cy, cz + nk * C::ROWS);
+          if (nk != hold)
+            Loader<C>::issue(g, ring, ptx::smem_addr(&bars[slot]), slot, cx, cy, cz + nk * C::ROWS);
           issued = nk + 1;
         }
       }
     }
     if (abort_flag) {
-      // drain: wait (bounded) for the copies still in flight before leaving
+      // drain: every copy this CTA requested must land before it exits (the
+      // copies write its shared memory).  The bound is fixed and generous,
+      // independent of the caller's timeout_ns, so a short caller limit ends
+      // the waits for input but never the drain; the chunk withheld by the
+      // failure-test hook was never requested and is skipped.
       if (threadIdx.x == 0) {
         for (int k = waited; k < issued; ++k) {
+          if (k == hold) continue;
           const unsigned gq = seq + k;
-          ptx::mbar_wait(ptx::smem_addr(&bars[gq % C::NSLOT]), (gq / C::NSLOT) & 1u, p.timeout_ns);
+          ptx::mbar_wait(ptx::smem_addr(&bars[gq % C::NSLOT]), (gq / C::NSLOT) & 1u, kDrainNs);
         }
       }
       __syncthreads();

@@ -110,7 +110,8 @@ typedef struct __attribute__((aligned(64))) csd_params {
   int ngrids;
   int total_items;
   int* err;                           // device error word (0 = ok)
-  unsigned long long timeout_ns;      // bound on every wait
+  unsigned long long timeout_ns;      // bound on every wait for input
+  int withhold;                       // failure-test hook (csd_launch_opts::withhold_chunk)
 } csd_params;
 
 // Compile-time configuration of a kernel, exported by each JIT module as

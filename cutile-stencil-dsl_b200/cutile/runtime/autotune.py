@@ -88,12 +88,14 @@ def _save(key: str, entry: dict) -> None:
 
 
 def candidates(ndim: int, dtype_bytes: int, radius, num_inputs: int, num_loads: int,
-               body_ops: int, single_field: bool, max_candidates: int = 30) -> list:
+               body_ops: int, single_field: bool, max_candidates: int = 30,
+               num_outputs: int = 1) -> list:
     """Distinct fitted plans around the default one, most promising first."""
     from cutile.passes.tiling import EnginePlan, default_engine_plan, fit_plan
 
     vec = 16 // dtype_bytes
-    base = default_engine_plan(ndim, num_loads, dtype_bytes, tuple(radius), num_inputs)
+    base = default_engine_plan(ndim, num_loads, dtype_bytes, tuple(radius), num_inputs,
+                               num_outputs)
     raw = [base]
     depths = (1, 2) if single_field else (1,)
     if ndim == 3:
@@ -125,12 +127,20 @@ def candidates(ndim: int, dtype_bytes: int, radius, num_inputs: int, num_loads: 
             continue
         if f.rows < radius[0] if ndim > 1 else False:
             continue
-        key = (f.rows, f.tile_y, f.tile_x, f.threads, f.stages, f.temporal, f.min_blocks)
+        key = (f.rows, f.tile_y, f.tile_x, f.threads, f.stages, f.temporal, f.min_blocks, f.rpy)
         if key in seen:
             continue
         seen.add(key)
         out.append(f)
     return out[:max_candidates]
+
+
+def probe_hints(p) -> dict:
+    """The kernel hints that make ``compile(tile_sizes=p.tile_sizes(), ...)``
+    build exactly the candidate plan ``p`` (rows per thread included), so the
+    plan that is timed is the plan that is returned."""
+    return {"threads": p.threads, "stages": p.stages, "zchunk": p.zchunk,
+            "min_blocks": p.min_blocks, "waves": p.waves, "rows_per_thread": p.rpy}
 
 
 def _gpu_name() -> str:
@@ -177,7 +187,7 @@ def autotune(stencil_fn, domain=None, hw=None, *, dtype: str | None = None,
                                   hit.get("candidates", 0))
     single = fp["inputs"] == 1 and fp["outputs"] == 1
     plans = candidates(ndim, dtype_bytes, fp["radius"], fp["inputs"], fp["loads"],
-                       fp["body_ops"], single, max_candidates)
+                       fp["body_ops"], single, max_candidates, fp["outputs"])
     if not torch.cuda.is_available():
         raise RuntimeError("autotune times candidates on the GPU; no CUDA device is visible")
     pts = 1
@@ -187,8 +197,7 @@ def autotune(stencil_fn, domain=None, hw=None, *, dtype: str | None = None,
 
     def probe(cfg: Config):
         p = plans[cfg.kernel_hints["_index"]]
-        hints = {"threads": p.threads, "stages": p.stages, "zchunk": p.zchunk,
-                 "min_blocks": p.min_blocks, "waves": p.waves}
+        hints = probe_hints(p)
         try:
             r = stencil_compile(stencil_fn, tile_sizes=p.tile_sizes(), kernel_hints=hints,
                                 temporal_steps=p.temporal, dtype=dtype, autotune=False,

@@ -337,8 +337,12 @@ def _plan_from(tile_sizes, kernel_hints, ndim, base_plan):
         for k in ("threads", "stages", "zchunk", "waves"):
             if k in kernel_hints:
                 kw[k] = int(kernel_hints[k])
-        if "rows_per_thread" in kernel_hints:
-            kw["rpy"] = int(kernel_hints["rows_per_thread"])
+        # "rows_per_thread" is the documented hint; "rpy" is the key
+        # EnginePlan.hints() writes (autotune results, caches), read back
+        # the same way so a tuned plan round-trips through compile()
+        for key in ("rpy", "rows_per_thread"):
+            if key in kernel_hints:
+                kw["rpy"] = int(kernel_hints[key])
         occ = kernel_hints.get("min_blocks", kernel_hints.get("occupancy"))
         if occ is not None:
             kw["occupancy"] = int(occ)
@@ -512,7 +516,8 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
     if align_halo and layout != "bricked":
         halo_widths = pad_inner_halo(halo_widths, dtype_bytes)
 
-    plan = default_engine_plan(len(stencil_halo), num_loads, dtype_bytes, stencil_halo, num_inputs)
+    plan = default_engine_plan(len(stencil_halo), num_loads, dtype_bytes, stencil_halo, num_inputs,
+                               _yields(ir))
     resources = None
     if autotune and domain is not None:
         from cutile.runtime.autotune import autotune as _autotune
@@ -784,7 +789,7 @@ def build_variants(stencil_fn, variants: dict, *, dtype: str | None = None,
             extra_in = ((m if rk["a"] != 0.0 and not rk.get("same_base") else 0)
                         + (m if rk.get("w") is not None else 0))
         plan = default_engine_plan(len(stencil_halo), num_loads, dtype_bytes, stencil_halo,
-                                   n_fields + extra_in)
+                                   n_fields + extra_in, _yields(ir))
         bmode = opts.pop("boundary_mode", "none")
         plan = fit_plan(_plan_from(tile_sizes, kernel_hints, len(stencil_halo), plan),
                         stencil_halo, dtype_bytes, n_fields + extra_in,

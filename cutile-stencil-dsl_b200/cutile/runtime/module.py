@@ -97,9 +97,15 @@ class StencilProgram:
 
     def launch(self, inputs, outputs, stream=None, *, zchunk: int = 0, grid: int = 0,
                loader: int = -1, scalars: dict | None = None, which: str = "main",
-               dyn=None, red=None, bc_odd=()) -> None:
+               dyn=None, red=None, bc_odd=(), timeout_ns: int = 0,
+               withhold_chunk: int = 0) -> None:
         """``launch_<name>``: ``temporal_steps`` steps from ``inputs`` into the
-        interiors of ``outputs`` (halos untouched)."""
+        interiors of ``outputs`` (halos untouched).
+
+        ``timeout_ns`` bounds every device wait for input (0: 2 s); a wait
+        that runs out stops its CTA and sets the device error word
+        (``native.error_word``).  ``withhold_chunk`` is the failure-test hook
+        of ``csd_launch_opts`` (one input chunk of CTA 0 is never requested)."""
         self._check(list(inputs) + list(outputs), "stencil")
         if len(inputs) != self.spec["inputs"] or len(outputs) != self.spec["outputs"]:
             raise TypeError(f"launch_{self.spec['name']} takes {self.spec['inputs']} input(s) and "
@@ -110,7 +116,8 @@ class StencilProgram:
                     raise ValueError("outputs must not alias inputs (the kernel reads neighbours)")
         native.launch(self.kernel(which), inputs, outputs, self.spec["halo"], stream,
                       zchunk=zchunk, grid=grid, loader=loader,
-                      scalars=self.scalar_values(scalars), dyn=dyn, red=red, bc_odd=bc_odd)
+                      scalars=self.scalar_values(scalars), dyn=dyn, red=red, bc_odd=bc_odd,
+                      timeout_ns=timeout_ns, withhold_chunk=withhold_chunk)
 
     def step(self, inputs, outputs, stream=None, *, scalars: dict | None = None, **kw) -> None:
         """One step with the declared boundary condition fused into staging:

@@ -36,7 +36,12 @@ NVRTC_OPTIONS = (
 
 
 class CsdError(RuntimeError):
-    """A libcsd call failed; the message is ``csd_last_error()``."""
+    """A libcsd call failed; the message is ``csd_last_error()`` and ``code``
+    the status (``CSD_E*`` in include/csd.h)."""
+
+    def __init__(self, msg: str, code: int = 0):
+        super().__init__(msg)
+        self.code = code
 
 
 class Field(ctypes.Structure):
@@ -53,7 +58,8 @@ class LaunchOpts(ctypes.Structure):
                 ("loader", ctypes.c_int), ("bc_value", ctypes.c_double),
                 ("timeout_ns", ctypes.c_uint64), ("scalars", ctypes.c_double * MAX_SCALARS),
                 ("dyn", ctypes.c_void_p), ("red", ctypes.c_void_p),
-                ("bc_odd", ctypes.c_int * MAX_FIELDS), ("grid_index", ctypes.c_void_p)]
+                ("bc_odd", ctypes.c_int * MAX_FIELDS), ("grid_index", ctypes.c_void_p),
+                ("withhold_chunk", ctypes.c_int)]
 
 
 class KernelDesc(ctypes.Structure):
@@ -143,7 +149,7 @@ def library() -> ctypes.CDLL:
 def check(rc: int) -> None:
     if rc != 0:
         msg = library().csd_last_error().decode(errors="replace")
-        raise CsdError(f"libcsd error {rc}: {msg}")
+        raise CsdError(f"libcsd error {rc}: {msg}", rc)
 
 
 def _headers():
@@ -325,8 +331,10 @@ def stream_handle(stream) -> int | None:
 
 
 def make_opts(halo, *, zchunk: int = 0, grid: int = 0, loader: int = -1, bc_value: float = 0.0,
-              timeout_ns: int = 0, scalars=(), dyn=None, red=None, bc_odd=()) -> LaunchOpts:
+              timeout_ns: int = 0, scalars=(), dyn=None, red=None, bc_odd=(),
+              withhold_chunk: int = 0) -> LaunchOpts:
     o = LaunchOpts()
+    o.withhold_chunk = withhold_chunk
     for i, h in enumerate(halo):
         o.halo[i] = int(h)
     o.zchunk = zchunk
@@ -501,14 +509,28 @@ def launch_fields(kernel: NativeKernel, fin, fout, halo, stream=None, **kw) -> N
                          ctypes.c_void_p(stream_handle(stream))))
 
 
-def error_word(reset: bool = True) -> int:
+CSD_ETIMEOUT = 5
+CSD_ERR_TIMEOUT = 0x7001
+
+
+def error_status(reset: bool = True) -> tuple[int, int]:
+    """``(status, word)`` of ``csd_error_word``: status CSD_OK for a clear
+    word, CSD_ETIMEOUT when a kernel's wait for input ran out; other
+    statuses raise."""
     v = ctypes.c_int()
-    check(library().csd_error_word(ctypes.byref(v), 1 if reset else 0))
-    return v.value
+    rc = library().csd_error_word(ctypes.byref(v), 1 if reset else 0)
+    if rc not in (0, CSD_ETIMEOUT):
+        check(rc)
+    return rc, v.value
+
+
+def error_word(reset: bool = True) -> int:
+    """The device error word (0 = no kernel reported a failure)."""
+    return error_status(reset)[1]
 
 
 __all__ = ["library", "check", "compile_source", "NativeModule", "NativeKernel", "launch",
-           "apply_boundary", "error_word", "CsdError", "field_of", "default_cache_dir",
+           "apply_boundary", "error_word", "error_status", "CSD_ETIMEOUT", "CSD_ERR_TIMEOUT", "CsdError", "field_of", "default_cache_dir",
            "make_opts", "grid_size", "grid_build", "launch_batch", "bricked_shape",
            "to_bricks", "from_bricks", "bricked_field", "launch_fields",
            "GridHead", "plan_items", "NVCC_OPTIONS", "find_nvcc", "aot_compile", "read_image", "CSD_LOADER_TMA", "CSD_LOADER_LDG", "BC_MODES"]

@@ -6,7 +6,7 @@
  * cutile/lowering/target_to_python.py:356-399) and CuPy slice copies for
  * boundaries (target_to_python.py:199-297).  This header is the boundary
  * that replaces those calls.  Each entry point cites the reference interface
- * it stands in for; INTEGRATION.md shows how a caller binds it.
+ * it stands in for, or says that it has none.
  *
  * Conventions: every function returns 0 on success or a CSD_E* code; the
  * message of the last failure on the calling thread is csd_last_error().
@@ -65,6 +65,11 @@ typedef struct csd_launch_opts {
   const int* grid_index;  /* csd_launch_batch: device map from batch position to descriptor
                              index in `grids` (NULL = identity), so descriptors can stay
                              resident in a pool while the batch changes */
+  int withhold_chunk;   /* failure-test hook (0 = off): the first work item of CTA 0 never
+                           requests input chunk withhold_chunk - 1, so its wait runs out after
+                           timeout_ns; the CTA drains its other copies and exits, and
+                           csd_error_word then reports CSD_ERR_TIMEOUT.  Nothing faults or
+                           hangs: every other CTA finishes normally. */
 } csd_launch_opts;
 
 /* Library version (major*100 + minor). */
@@ -190,7 +195,9 @@ int csd_reduce(const csd_field* a, const csd_field* b, const int* halo, int op,
  * CSD_NOALLOC_MAX_BLOCKS = 1024 doubles (8 KB) that every device keeps until
  * the process exits; `nblocks` above 1024 is rejected with CSD_EINVAL.  The
  * first call on a device looks up the array's device address (with that
- * device current); make that first call before any stream capture.  Calls
+ * device current); make that first call before any stream capture.  After
+ * cudaDeviceReset the device has a new context and the next call looks the
+ * address up again, so that call too belongs before any capture.  Calls
  * share the array, so calls that overlap on the GPU race; each call
  * overwrites the partials it uses, so no clearing is needed.  Nothing is
  * allocated.  No counterpart in the reference. */
@@ -211,7 +218,10 @@ int csd_to_bricks(const csd_field* flat, int brick, void* bricked, void* stream)
 int csd_from_bricks(const void* bricked, int brick, const csd_field* flat, void* stream);
 
 /* Read (and with reset != 0, clear) the device error word of the current
- * device; synchronises the device. */
+ * device; synchronises the device.  `value` receives the word (0, or
+ * CSD_ERR_TIMEOUT when a kernel's wait for its input ran out: that CTA
+ * drained its copies in flight and stopped, so its outputs are incomplete).
+ * Returns CSD_OK for a clear word, CSD_ETIMEOUT for CSD_ERR_TIMEOUT. */
 int csd_error_word(int* value, int reset);
 
 #ifdef __cplusplus

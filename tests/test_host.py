@@ -411,3 +411,88 @@ def test_rows_per_thread_plans():
         fit_plan(replace(p, temporal=2), (1, 1, 1), 8, 1)
     with pytest.raises(ValueError):
         fit_plan(replace(p, tile_y=6, rpy=4), (1, 1, 1), 8, 1)
+
+
+# --------------------------------------------------------------------------- #
+# Autotune plans round-trip through compile()
+# --------------------------------------------------------------------------- #
+
+
+def _box27():
+    import wide_defs as W
+
+    return W.load_box("box27_rt", 1)
+
+
+def test_probe_compiles_the_candidate_plan():
+    """Every autotune candidate, compiled with the hints its probe passes,
+    gives a kernel of that plan (rows per thread included)."""
+    import cutile
+    from cutile.runtime import autotune as A
+
+    fn = _box27()
+    fp = A._footprint(fn, 8)
+    plans = A.candidates(3, 8, fp["radius"], fp["inputs"], fp["loads"], fp["body_ops"],
+                         True, 30, fp["outputs"])
+    assert any(p.rpy > 1 for p in plans), "the rows-per-thread default is a candidate"
+    for p in plans:
+        r = cutile.compile(fn, tile_sizes=p.tile_sizes(), kernel_hints=A.probe_hints(p),
+                           temporal_steps=p.temporal, autotune=False)
+        assert r.tile_sizes == p.tile_sizes()
+        assert r.kernel_hints == p.hints(), (p, r.kernel_hints)
+
+
+def test_candidates_keep_plans_that_differ_only_in_rows_per_thread():
+    from dataclasses import replace
+
+    from cutile.passes.tiling import default_engine_plan
+
+    base = default_engine_plan(3, 27, 8, (1, 1, 1), 1, 1)
+    assert base.rpy == 4
+    key = lambda f: (f.rows, f.tile_y, f.tile_x, f.threads, f.stages, f.temporal, f.min_blocks, f.rpy)
+    assert key(base) != key(replace(base, rpy=1))
+
+
+def test_autotuned_hints_round_trip_through_compile():
+    """An AutotuneResult's (tile_sizes, kernel_hints) passed back to compile()
+    rebuild its plan: the 'rpy' key written by EnginePlan.hints() is read."""
+    import cutile
+    from cutile.passes.tiling import default_engine_plan
+
+    fn = _box27()
+    plan = default_engine_plan(3, 27, 8, (1, 1, 1), 1, 1)
+    r0 = cutile.compile(fn, temporal_blocking=False, autotune=False)
+    assert r0.kernel_hints.get("rpy") == plan.rpy == 4
+    r1 = cutile.compile(fn, tile_sizes=r0.tile_sizes, kernel_hints=r0.kernel_hints,
+                        temporal_blocking=False, autotune=False)
+    assert r1.kernel_hints == r0.kernel_hints and r1.tile_sizes == r0.tile_sizes
+
+
+def test_tuple_returning_stencil_keeps_one_row_per_thread():
+    """The rows-per-thread default is for one-input, one-output kernels; a
+    wide single-input stencil with two outputs keeps one row."""
+    import cutile
+    from cutile import stencil
+
+    def two(u, i, j, k):
+        s = (u[i - 1, j, k] + u[i + 1, j, k] + u[i, j - 1, k] + u[i, j + 1, k] + u[i, j, k - 1]
+             + u[i, j, k + 1] + u[i - 1, j - 1, k] + u[i + 1, j + 1, k] + u[i - 1, j, k - 1]
+             + u[i + 1, j, k + 1] + u[i, j - 1, k - 1] + u[i, j + 1, k + 1] + u[i - 1, j + 1, k]
+             + u[i + 1, j - 1, k] + u[i, j - 1, k + 1] + u[i, j + 1, k - 1] + u[i - 1, j, k + 1])
+        return s, 0.5 * s
+
+    import importlib.util
+    import inspect
+    import os
+    import tempfile
+    import textwrap
+
+    src = "from cutile import stencil\n\n@stencil(ndim=3)\n" + textwrap.dedent(inspect.getsource(two))
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "two_out.py")
+        open(path, "w").write(src)
+        spec = importlib.util.spec_from_file_location("two_out", path)
+        m = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(m)
+        r = cutile.compile(m.two, temporal_blocking=False, autotune=False)
+    assert "rpy" not in r.kernel_hints

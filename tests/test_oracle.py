@@ -89,3 +89,38 @@ def test_bricks_round_trip():
     b = O.to_bricks(a, 4)
     assert b.shape == (3, 4, 2, 4, 4, 4)
     assert np.array_equal(O.from_bricks(b, a.shape, 4), a)
+
+
+# --------------------------------------------------------------------------- #
+# The reference-test corpus: every @stencil of the reference's tests plus its
+# random-expression generator's cases, as evaluated by the reference's own
+# executor (tests/ref_corpus.py, tests/golden/make_golden.py)
+# --------------------------------------------------------------------------- #
+
+import ref_corpus as RC  # noqa: E402
+
+_CORPUS, _CORPUS_OUT = RC.load()
+
+
+@pytest.mark.parametrize("key", sorted(_CORPUS))
+def test_oracle_matches_reference_corpus(tmp_path, key):
+    e = _CORPUS[key]
+    fn = RC.build(tmp_path, key, e)
+    ins = RC.inputs(e)
+    dt = np.float32 if e["dtype"] == "float32" else np.float64
+    got = O.evaluate(dict(zip(e["args"], ins)), fn, e["ndim"], tuple(e["halo"]), tuple(e["shape"]), dt)
+    want = _CORPUS_OUT[key]
+    got = np.broadcast_to(np.asarray(got, dt), want.shape)
+    assert got.dtype == want.dtype and np.array_equal(got, want), e["origin"]
+
+
+def test_corpus_covers_the_reference_suites():
+    """The fixture holds the application set, the wide boxes, the precedence
+    and element-wise math cases and the generator's 47 distinct cases."""
+    origins = {e["origin"].split(":")[0] for e in _CORPUS.values()}
+    for f in ("tests/test_cutile_gpu_apps.py", "tests/wide_stencils.py", "tests/test_expr_precedence.py",
+              "tests/test_frontend_math.py", "tests/test_term_order.py", "tests/test_exact_constants.py",
+              "tests/random_stencils.py"):
+        assert f in origins
+    assert sum(k.startswith("random_stencils/") for k in _CORPUS) == 47
+    assert {"wide_stencils/box125", "wide_stencils/box27"} <= set(_CORPUS)
