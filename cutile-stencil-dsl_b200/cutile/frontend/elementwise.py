@@ -4,7 +4,7 @@ Inside a ``@stencil`` body the parser lowers ``max``/``min``/``abs``/``where``
 (and ``sqrt``) to IR ops.  When the same Python function runs on NumPy or
 torch arrays (``CompileResult.validate``), the builtins ``max``/``min`` reject
 arrays, so these dispatch to the array library of their operands, as the
-reference's ``cutile.reference.elementwise`` does (elementwise.py:262-297).
+reference's ``cutile.reference.elementwise`` does (elementwise.py:17-52).
 """
 
 from __future__ import annotations

@@ -1,9 +1,12 @@
 """Bricked layout tag (reference: cutile/passes/bricked.py:24-46).
 
-Attaches ``layout = "bricked"`` and ``brick_size`` to each apply.  On the
-B200 backend a bricked stencil is stored brick-major (``cutile.dialects.
-layout.LayoutAttr``) and the engine stages whole bricks with one TMA copy
-each, instead of the reference's flat round-trip.
+Attaches ``layout = "bricked"`` and ``brick_size`` to each apply (the
+attributes the reference's pass writes).  ``compile(layout="bricked")``
+itself passes the layout to the lowering directly: on the B200 backend the
+fields can stay resident brick-major (``cutile.dialects.layout.LayoutAttr``)
+and the engine's bricked instantiation addresses bricks when it stages
+chunks, stores outputs and patches boundaries, instead of the reference's
+flat round-trip around a flat kernel.
 """
 
 from __future__ import annotations

@@ -1,6 +1,6 @@
 """Normalization: Dialect 1 -> standard ``stencil`` dialect (Dialect 2).
 
-Follows cutile/lowering/normalize.py:111-221: every ``cutile_stencil.func``
+Follows cutile/lowering/normalize.py:47-156: every ``cutile_stencil.func``
 becomes ``func.func`` wrapping one ``stencil.apply`` whose body has one
 ``TempType`` argument per input array, ``stencil.access`` per D1 access, the
 cloned arith/math ops and ``stencil.return``.  ``ndim``, ``order``, ``dtype``,

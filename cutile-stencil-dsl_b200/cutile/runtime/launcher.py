@@ -34,6 +34,7 @@ from dataclasses import dataclass, field, replace
 from typing import Any, Optional
 
 from cutile.dialects.stencil import ApplyOp
+from cutile.passes.verify import verify_engine_plan
 from cutile.runtime.pipeline import Pipeline
 
 
@@ -542,6 +543,7 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
     if occupancy is not None:
         plan = replace(plan, occupancy=int(occupancy))
     plan = fit_plan(plan, stencil_halo, dtype_bytes, num_inputs, analysis.get("body_ops", 0))
+    verify_engine_plan(clone, plan, stencil_halo, dtype_bytes, num_inputs)
     hints = plan.hints()
     if occupancy is not None:
         hints["occupancy"] = occupancy
@@ -561,6 +563,8 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
     if boundary_spec is not None:
         bc_plan = fit_plan(replace(plan, temporal=1), stencil_halo, dtype_bytes, num_inputs,
                            analysis.get("body_ops", 0),
+                           periodic=boundary_spec.get("type") == "periodic")
+        verify_engine_plan(clone, bc_plan, stencil_halo, dtype_bytes, num_inputs,
                            periodic=boundary_spec.get("type") == "periodic")
         bc_target = lower_to_target_ir(ir.clone(), bc_plan.tile_sizes(), halo_widths,
                                        temporal_steps=1, boundary_spec=boundary_spec,
@@ -699,6 +703,11 @@ def compile_fused(stencil_fns: list, domain: tuple[int, ...] | None = None, hw=N
         plan = replace(plan, occupancy=int(occupancy))
     body_ops = sum(sum(1 for _ in m.walk()) for m in modules)
     plan = fit_plan(plan, stencil_halo, dtype_bytes, meta.num_inputs, body_ops)
+    for m in modules:
+        c = m.clone()
+        Pipeline.single_gpu(dtype_bytes=dtype_bytes, max_temporal_steps=1).run(c)
+        verify_engine_plan(c, plan, stencil_halo, dtype_bytes, meta.num_inputs,
+                           periodic=boundary == "periodic")
     hints = plan.hints()
     if occupancy is not None:
         hints["occupancy"] = occupancy
@@ -794,6 +803,8 @@ def build_variants(stencil_fn, variants: dict, *, dtype: str | None = None,
         plan = fit_plan(_plan_from(tile_sizes, kernel_hints, len(stencil_halo), plan),
                         stencil_halo, dtype_bytes, n_fields + extra_in,
                         analysis.get("body_ops", 0), periodic=bmode == "periodic")
+        verify_engine_plan(clone, plan, stencil_halo, dtype_bytes, n_fields + extra_in,
+                           periodic=bmode == "periodic")
         target = lower_to_target_ir(ir.clone(), plan.tile_sizes(), tuple(halo_widths),
                                     kernel_hints=plan.hints(), dtype=dtype, name=kname,
                                     boundary_spec=bspec, boundary_mode=bmode, **opts)

@@ -8,7 +8,7 @@ A NumPy restatement of the reference's executor and launcher semantics:
 
 * ``apply_stencil``  -- reference/stencil_ref.py:52-87 (``_ArrayProxy``
   shifted interior views, builtins max/min swapped for array versions as in
-  reference/elementwise.py:285-297; a copy of ``u`` with only the interior
+  reference/elementwise.py:40-52; a copy of ``u`` with only the interior
   replaced);
 * ``apply_boundary`` -- reference/stencil_ref.py:102-201 (per dimension,
   low side then high side, Dirichlet / Neumann / periodic / reflecting);
@@ -38,7 +38,7 @@ import numpy as np
 
 
 # --------------------------------------------------------------------------- #
-# Array-aware helpers (reference/elementwise.py:262-297)
+# Array-aware helpers (reference/elementwise.py:17-52)
 # --------------------------------------------------------------------------- #
 
 
