@@ -885,6 +885,97 @@ def run_gray_scott(args) -> dict | None:
     return line if rank == 0 else None
 
 
+# ---------------------------------------------------------------------------
+# Small-step heat diffusion: where the compensated FP32 update pays
+# ---------------------------------------------------------------------------
+HEAT_METRIC = "GPts/s (2-D heat, small step, FP32 + Kahan)"
+
+
+def run_heat_kahan(args) -> dict | None:
+    """2-D heat u += 0.02 * lap(u), 4096^2, zero Dirichlet halo, u = 1 + 0.1
+    * Gaussian bump: every update is ~1e-8..1e-4 of u, below FP32's rounding
+    of u in most of the field.  FP64, FP32 and FP32+Kahan run the same steps
+    from the same start; the line reports the Kahan kernel's throughput and
+    each FP32 mode's relative L2 error against FP64."""
+    import numpy as np
+    import torch
+
+    import cutile
+    import stencil_defs as D
+    from cutile import stencil
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    n, steps = GS_N, args.steps
+    stream = torch.cuda.current_stream()
+    runs = {}
+    for prec in ("fp64", "fp32", "fp32_kahan"):
+        dt = "float64" if prec == "fp64" else "float32"
+        r = cutile.compile(stencil(ndim=2, dtype=dt)(D.heat_small_dt), precision=prec,
+                           temporal_blocking=False)
+        h = r.halo_widths
+        u0 = D.heat_bump_init(n, halo=h, dtype=dt)
+        launch = getattr(r.load_module(), f"launch_{r.name}")
+        a = torch.from_numpy(u0).cuda()
+        b = torch.zeros_like(a)
+        ca, cb = torch.zeros_like(a), torch.zeros_like(a)
+        kahan = prec == "fp32_kahan"
+        for _ in range(args.warmup):
+            launch(a, ca, b, cb) if kahan else launch(a, b)
+        a.copy_(torch.from_numpy(u0))
+        ca.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        clk = ClockSampler(local).__enter__() if kahan else None
+        e0.record(stream)
+        for _ in range(steps):
+            if kahan:
+                launch(a, ca, b, cb)
+                ca, cb = cb, ca
+            else:
+                launch(a, b)
+            a, b = b, a
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clocks = None
+        if kahan:
+            clk.__exit__(None, None, None)
+            clocks = clk.summary()
+        inner = tuple(slice(x, sz - x) for x, sz in zip(h, u0.shape))
+        runs[prec] = {"ms": e0.elapsed_time(e1), "u": a[inner].double(), "clocks": clocks}
+        del a, b, ca, cb
+
+    def rel(x, y):
+        return float(torch.linalg.norm(x - y) / torch.linalg.norm(y))
+
+    ref = runs["fp64"]["u"]
+    err = {p: rel(runs[p]["u"], ref) for p in ("fp32", "fp32_kahan")}
+    npts = n * n
+    gpts = {p: npts * steps / (runs[p]["ms"] / 1e3) / 1e9 for p in runs}
+    ms_step = runs["fp32_kahan"]["ms"] / steps
+    alg = 4 * 4 * npts     # u, c read and written, FP32
+    peak, peak_kind = _peaks()
+    line = {
+        "metric": HEAT_METRIC, "value": round(gpts["fp32_kahan"], 3), "unit": "GPts/s",
+        "n_gpus": 1, "steps": steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 5),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 + f32 compensation", "data": "synthetic",
+        "config": {"workload": f"2-D heat u + 0.02*(N+S+W+E-4u), {n}^2, zero Dirichlet halo, "
+                               f"u = 1 + 0.1*Gaussian bump (width 0.08); {steps} steps from the "
+                               f"initial state, FP64 / FP32 / FP32+Kahan"},
+        "comparison": {"fp64_gpts": round(gpts["fp64"], 3), "fp32_gpts": round(gpts["fp32"], 3),
+                       "fp32_kahan_gpts": round(gpts["fp32_kahan"], 3),
+                       "rel_l2_vs_fp64_after_steps": err},
+        "roofline": {"bound": "hbm", "achieved": round(alg / (ms_step / 1e3) / 1e9, 1),
+                     "peak": peak, "unit": "GB/s",
+                     "frac": round(alg / (ms_step / 1e3) / 1e9 / peak, 4), "traffic": None,
+                     "peak_kind": peak_kind, "algorithmic_bytes_per_launch": alg},
+        "gpu_launches": steps, "clocks": runs["fp32_kahan"]["clocks"], "cpu_baseline": None,
+    }
+    return line if rank == 0 else None
+
+
 def run_gs_reference(args) -> dict | None:
     world, rank, _ = _dist()
     if rank != 0:
@@ -1018,6 +1109,25 @@ def run_serve(args) -> dict | None:
         solves_s = len(done) * world / _max_over_ranks(span)
     gpts = _serve_point_steps([r for r in reqs]) / span / 1e9
 
+    # the same mix at an arrival rate the server sustains (half its measured
+    # throughput), so that p50/p99 describe the server rather than a queue
+    # that grows for the whole run
+    sus_rate = max(50.0, 0.5 * solves_s)
+    sus_reqs = _serve_workload(max(200, SERVE_REQUESTS // 2), rate=sus_rate, seed=40 + rank)
+    sus_res = server.run(sus_reqs, realtime=True, keep_state=False)
+    torch.cuda.synchronize()
+    server.stats = type(server.stats)()
+    sus_done = [r for r in sus_res if r.error is None]
+    sus_lat = [r.latency * 1e3 for r in sus_done]
+    sus_span = max(r.completed for r in sus_done) - min(r.arrival for r in sus_reqs)
+    sustained = {"rate_req_s": round(sus_rate, 1), "requests": len(sus_reqs),
+                 "solves_s": round(len(sus_done) / sus_span, 3),
+                 "latency_ms": {"p50": round(percentile(sus_lat, 50), 3),
+                                "p99": round(percentile(sus_lat, 99), 3),
+                                "mean": round(float(np.mean(sus_lat)), 3)},
+                 "note": "Poisson arrivals at half the throughput measured under the "
+                         f"{SERVE_RATE:.0f} req/s stream (seed 40), same request mix"}
+
     # each request alone on the plain path (drop-in launch per step), sampled
     rng = np.random.default_rng(7)
     sample = sorted(rng.choice(len(reqs), size=min(64, len(reqs)), replace=False).tolist())
@@ -1071,6 +1181,7 @@ def run_serve(args) -> dict | None:
         "latency_ms": {"p50": round(percentile(lat, 50), 3), "p99": round(percentile(lat, 99), 3),
                        "mean": round(float(np.mean(lat)), 3)},
         "comparison": {
+            "sustained_rate": sustained,
             "alone_plain_solves_s": round(1e3 / alone_mean, 3),
             "speedup_vs_alone_plain": round(solves_s / (1e3 / alone_mean), 3),
             "alone_sequential_latency_ms": {"p50": round(percentile(seq_lat, 50), 3),
@@ -1235,6 +1346,76 @@ def run_sw_reference(args) -> dict | None:
     }
 
 
+# Secondary workloads the default run reports beside the headline: each runs
+# as its own `bench.py` process (its own memory, its own clock samples) and
+# contributes a compact summary of its JSON line under "secondary".
+SECONDARY = (
+    ("lap7_fp32", ["--dtype", "float32", "--steps", "20"]),
+    ("lap7_fp64_T2", ["--temporal", "2", "--steps", "20"]),
+    ("lap7_fp64_bricked8", ["--layout", "bricked", "--steps", "20"]),
+    ("gray_scott_4096_kahan", ["--workload", "gray_scott", "--steps", "1000"]),
+    ("heat_4096_small_step_kahan", ["--workload", "heat_kahan", "--steps", "2000"]),
+    ("sw_batch_256", ["--workload", "sw_batch"]),
+    ("wide", ["--workload", "wide"]),
+    ("serve", ["--workload", "serve"]),
+)
+_SUMMARY_KEYS = ("metric", "value", "unit", "steps", "ms_per_step", "dtype", "latency_ms",
+                 "comparison")
+
+
+def _summary(line: dict) -> dict:
+    """The figures of a workload line worth carrying beside the headline."""
+    out = {k: line[k] for k in _SUMMARY_KEYS if k in line}
+    server = (out.get("comparison") or {}).get("server")
+    if isinstance(server, dict):
+        out["comparison"] = dict(out["comparison"],
+                                 server={k: v for k, v in server.items() if k != "timeline"})
+    cfg = line.get("config") or {}
+    out["workload"] = cfg.get("workload")
+    for k in ("temporal_steps", "tile", "layout"):
+        if k in cfg:
+            out[k] = cfg[k]
+    rf = line.get("roofline")
+    if rf:
+        out["roofline"] = {k: rf.get(k) for k in ("bound", "achieved", "peak", "unit", "frac",
+                                                 "traffic", "algorithmic_bytes_per_launch")
+                           if k in rf}
+    if line.get("e2e"):
+        out["e2e"] = {"value": line["e2e"].get("value"), "unit": line["e2e"].get("unit")}
+    if line.get("clocks"):
+        c = line["clocks"]
+        out["clocks"] = {k: c.get(k) for k in ("sm_mhz", "sm_max_mhz", "reasons")}
+    if line.get("gpu_launches") is not None:
+        out["gpu_launches"] = line["gpu_launches"]
+    return out
+
+
+def run_secondary(budget_s: float = 600.0) -> dict:
+    """Run each secondary workload in a child process and summarise it."""
+    res = {}
+    t_end = time.monotonic() + budget_s
+    for name, extra in SECONDARY:
+        left = t_end - time.monotonic()
+        if left < 30:
+            res[name] = {"skipped": "secondary time budget spent"}
+            continue
+        t0 = time.monotonic()
+        try:
+            p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--no-cpu"] + extra,
+                               capture_output=True, text=True, timeout=min(left, 300))
+        except subprocess.TimeoutExpired:
+            res[name] = {"error": "timed out"}
+            continue
+        lines = [l for l in p.stdout.splitlines() if l.startswith("{")]
+        if p.returncode != 0 or not lines:
+            tail = (p.stderr or p.stdout).strip().splitlines()[-1:] or [""]
+            res[name] = {"error": f"rc={p.returncode}: {tail[0][:200]}"}
+            continue
+        res[name] = _summary(json.loads(lines[-1]))
+        res[name]["wall_s"] = round(time.monotonic() - t0, 1)
+    return res
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1251,7 +1432,8 @@ def main() -> None:
     ap.add_argument("--gs-n", type=int, default=4096, help="gray_scott: interior extent")
     ap.add_argument("--serve-requests", type=int, default=2000,
                     help="serve: number of requests in the stream")
-    ap.add_argument("--workload", choices=("lap7", "sw_batch", "gray_scott", "serve", "wide"),
+    ap.add_argument("--workload", choices=("lap7", "sw_batch", "gray_scott", "serve", "wide",
+                                           "heat_kahan"),
                     default="lap7",
                     help="lap7: 3-D 7-point 512^3 sweeps; sw_batch: 256 batched shallow-water "
                          "solves; gray_scott: 4096^2 fused Gray-Scott, FP64/FP32/Kahan")
@@ -1263,6 +1445,9 @@ def main() -> None:
                     help="sw_batch: rows per work item (0: the kernels' default)")
     ap.add_argument("--no-compare", dest="compare", action="store_false",
                     help="sw_batch: time the FP32 batch only (profiling cases)")
+    ap.add_argument("--no-secondary", dest="secondary", action="store_false",
+                    help="default run: skip the secondary workloads summarised under "
+                         "'secondary' (each runs as its own process after the headline)")
     args = ap.parse_args()
     args.steps_given = args.steps
     if args.steps is None:
@@ -1288,6 +1473,14 @@ def main() -> None:
                     "(one launch per grid); the plain-path comparison is in the serve line"}
         else:
             line = run_serve(args)
+    elif args.workload == "heat_kahan":
+        if args.impl == "reference":
+            line = {"impl": "reference", "unavailable": "accuracy comparison of the GPU precision "
+                    "modes; its CPU side is the oracle's float32 Kahan step in the parity tests"}
+        else:
+            if args.steps_given is None:
+                args.steps = 2000
+            line = run_heat_kahan(args)
     elif args.workload == "gray_scott":
         if args.steps_given is None:
             args.steps = GS_STEPS if args.impl == "ours" else 3
@@ -1298,6 +1491,13 @@ def main() -> None:
         line = run_sw_reference(args) if args.impl == "reference" else run_sw_batch(args)
     else:
         line = run_reference(args) if args.impl == "reference" else run_ours(args)
+        default_run = (args.impl == "ours" and args.workload == "lap7" and args.dtype == "float64"
+                       and args.temporal == 1 and args.layout == "flat" and args.n == 512)
+        if (line is not None and default_run and args.secondary and line.get("n_gpus") == 1
+                and not args.no_cpu):
+            # the headline is complete (its timed region is over); the
+            # other configurations follow, each in its own process
+            line["secondary"] = run_secondary()
     if line is not None:
         print(json.dumps(line), flush=True)
 

@@ -53,6 +53,26 @@ def wave4(u, i, j):
             + WAVE_C * (4 / 3) * u[i, j + 1] + WAVE_C * (-1 / 12) * u[i, j + 2])
 
 
+# Heat diffusion with a small step (alpha * dt / dx^2 = 0.02): each update is
+# a tiny fraction of u, which is where a compensated FP32 update pays.
+KD_HEAT = 0.02
+
+
+def heat_small_dt(u, i, j):
+    return u[i, j] + KD_HEAT * (u[i - 1, j] + u[i + 1, j] + u[i, j - 1] + u[i, j + 1] - 4.0 * u[i, j])
+
+
+def heat_bump_init(n: int, halo=(1, 1), dtype="float64"):
+    """u = 1 + 0.1 * Gaussian bump (width 0.08) on an n x n interior, zero halo."""
+    import numpy as np
+
+    y = (np.arange(n) + 0.5) / n
+    r2 = (y[:, None] - 0.5) ** 2 + (y[None, :] - 0.45) ** 2
+    u = np.zeros((n + 2 * halo[0], n + 2 * halo[1]))
+    u[halo[0]:halo[0] + n, halo[1]:halo[1] + n] = 1.0 + 0.1 * np.exp(-r2 / (2 * 0.08 ** 2))
+    return u.astype(dtype)
+
+
 def leapfrog(u, up, i, j):
     return 2.0 * u[i, j] - up[i, j] + 0.25 * (u[i - 1, j] + u[i + 1, j] + u[i, j - 1]
                                               + u[i, j + 1] - 4.0 * u[i, j])
