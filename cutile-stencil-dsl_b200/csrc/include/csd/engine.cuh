@@ -30,6 +30,11 @@ namespace csd {
 
 // Bound on the drain of an aborted work item (copies still in flight).
 constexpr unsigned long long kDrainNs = 2000000000ull;
+// Stages with at most this many units per thread unroll their unit loop.
+#ifndef CSD_UNROLL_UNITS
+#define CSD_UNROLL_UNITS 4
+#endif
+constexpr int kUnrollUnits = CSD_UNROLL_UNITS;
 
 template <typename T>
 struct VecOf;
@@ -88,8 +93,10 @@ struct Cfg {
   static __host__ __device__ constexpr int ISLOT_ELEMS(int s) {
     return align_up(ROWS * H(s) * BOXW, 128 / (int)sizeof(T));
   }
-  static __host__ __device__ constexpr int inter_elems_upto(int s) {  // rings 1..s-1
-    return s <= 1 ? 0 : inter_elems_upto(s - 1) + NSLOT_I * ISLOT_ELEMS(s - 1);
+  // Intermediate rings of stages 1..s-1; each stage keeps one ring per field
+  // (a chain maps output field f to input field f of the next step).
+  static __host__ __device__ constexpr int inter_elems_upto(int s) {
+    return s <= 1 ? 0 : inter_elems_upto(s - 1) + NIN * NSLOT_I * ISLOT_ELEMS(s - 1);
   }
   static constexpr int RING_ELEMS = NIN * NSLOT * SLOT_ELEMS;
   static constexpr int INTER_ELEMS = inter_elems_upto(TEMPORAL);
@@ -109,7 +116,8 @@ struct Cfg {
   static constexpr int SMEM_BYTES = BAR_OFFSET + 8 * NSLOT + 64 + 128;
   static_assert(BOXW <= 256 && BOXH <= 256 && ROWS <= 256, "TMA box limit");
   static_assert(TX % VEC == 0, "tile width must be a multiple of the vector width");
-  static_assert(TEMPORAL == 1 || (NIN == 1 && NOUT == 1), "temporal chains need one field");
+  static_assert(TEMPORAL == 1 || NIN == NOUT,
+                "a temporal chain feeds output field f into input field f of the next step");
   static_assert(HC * ROWS >= RZ, "halo chunks");
   static_assert(BC == CSD_BC_NONE || TEMPORAL == 1, "fused boundary fill is single-step");
   static_assert(RPY >= 1 && TY % RPY == 0, "tile height must be a multiple of the rows per thread");
@@ -688,7 +696,9 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
           src.nslot = C::NSLOT;
           src.slot_elems = C::SLOT_ELEMS;
         } else {
-          src.base[0] = inter + C::inter_elems_upto(s - 1);
+#pragma unroll
+          for (int f = 0; f < C::NIN; ++f)
+            src.base[f] = inter + C::inter_elems_upto(s - 1) + f * C::NSLOT_I * C::ISLOT_ELEMS(s - 1);
           src.slot0 = c0 % C::NSLOT_I;
           src.nslot = C::NSLOT_I;
           src.slot_elems = C::ISLOT_ELEMS(s - 1);
@@ -716,8 +726,7 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
         const int ybuf0 = Y0 - (T_ - s) * C::RY;  // array row of dst buffer row 0
         T* dst = last ? nullptr
                       : inter + C::inter_elems_upto(s) + (k % C::NSLOT_I) * C::ISLOT_ELEMS(s);
-#pragma unroll 1
-        for (int u = threadIdx.x; u < units; u += C::NT) {
+        auto unit = [&](const int u) {
           const int xv = xv_lo + u % nxv;
           const int t2 = u / nxv;
           const int y = (t2 % hsu) * C::RPY;
@@ -780,15 +789,32 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
                 }
               }
             } else {
-              T* d = dst + (r * hs + y + j) * C::BOXW + xv * C::VEC;
+              // intermediate field(s): zero outside the domain interior, as
+              // the zero-halo scratch buffers of T separate launches hold
 #pragma unroll
-              for (int e = 0; e < C::VEC; ++e) {
-                const int gx = gx0 + e;
-                const bool in = zin && yin && gx >= hx && gx < hx + nx;
-                d[e] = in ? ov[0][e] : T(0);
+              for (int f = 0; f < C::NOUT; ++f) {
+                T* d = dst + f * C::NSLOT_I * C::ISLOT_ELEMS(s) + (r * hs + y + j) * C::BOXW +
+                       xv * C::VEC;
+#pragma unroll
+                for (int e = 0; e < C::VEC; ++e) {
+                  const int gx = gx0 + e;
+                  const bool in = zin && yin && gx >= hx && gx < hx + nx;
+                  d[e] = in ? ov[f][e] : T(0);
+                }
               }
             }
           }  // rows of the unit
+        };
+        // A short, exact count of units per thread is unrolled, so that the
+        // units' coordinates fold into per-thread constants; longer or
+        // ragged counts loop.
+        if (units % C::NT == 0 && units / C::NT <= kUnrollUnits) {
+#pragma unroll
+          for (int q = 0; q < kUnrollUnits; ++q)
+            if (q < units / C::NT) unit(threadIdx.x + q * C::NT);
+        } else {
+#pragma unroll 1
+          for (int u = threadIdx.x; u < units; u += C::NT) unit(u);
         }
         __syncthreads();
       }

@@ -205,8 +205,9 @@ def engine_geometry(plan: EnginePlan, radius3: tuple[int, int, int], dtype_bytes
     nslot_i = 2 * hc + 1
     per128 = 128 // dtype_bytes
     slot_elems = _align_up(plan.rows * box_h * box_w, per128)
-    inter = sum(nslot_i * _align_up(plan.rows * (plan.tile_y + 2 * (T - s) * ry) * box_w, per128)
-                for s in range(1, T))
+    inter = num_inputs * sum(nslot_i * _align_up(plan.rows * (plan.tile_y + 2 * (T - s) * ry) * box_w,
+                                                 per128)
+                             for s in range(1, T))
     wrapw = _align_up(rx, align) + align
     pbuf_slot = (num_inputs * 2 * _align_up(plan.rows * box_h * wrapw, per128)
                  if (periodic and rx > 0) else 0)

@@ -529,10 +529,14 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
         T = res.temporal_steps
     if kahan:
         num_inputs += 1  # the compensation field
+    n_out = _yields(ir) * (2 if kahan else 1)
     if temporal_steps is not None:
         T = int(temporal_steps)
-        if T > 1 and num_inputs != 1:
-            raise NotImplementedError("temporal blocking needs a single-field stencil")
+        if T > 1 and num_inputs != n_out:
+            # a chain feeds output field f into input field f of the next
+            # step (an extension: the reference chains one field only)
+            raise NotImplementedError("temporal blocking needs one output per input field "
+                                      "(output f feeds input f of the next step)")
     elif num_inputs != 1 or _yields(ir) > 1:
         # The reference's T-launch loop chains one field only
         # (stencil_to_target.py:796-800), so a multi-field stencil cannot run

@@ -223,6 +223,26 @@ def temporal_launch(u_in: np.ndarray, u_out: np.ndarray, fn, ndim: int, halo_wid
     return cur
 
 
+def kahan_temporal_launch(u_in, c_in, incr_fn, ndim: int, halo_widths, steps: int,
+                          u_out=None, c_out=None):
+    """One launch of a Kahan-compensated stencil with ``temporal_steps = steps``:
+    ``steps`` compensated updates (``kahan_update``) chained the way
+    ``temporal_launch`` chains a single field -- intermediate iterates of u and
+    of its compensation have zero halos -- with only the outputs' interiors
+    written.  Returns ``(u, c)``."""
+    inner = _interior(u_in.shape, halo_widths)
+    cu, cc = u_in, c_in
+    for s in range(steps):
+        inc = evaluate_ops({"u": cu}, incr_fn, ndim, halo_widths, u_in.shape, u_in.dtype)[0]
+        nu, nc = kahan_update(cu[inner], cc[inner], inc)
+        last = s == steps - 1
+        a = (u_out.copy() if u_out is not None else np.zeros_like(u_in)) if last else np.zeros_like(u_in)
+        b = (c_out.copy() if c_out is not None else np.zeros_like(c_in)) if last else np.zeros_like(c_in)
+        a[inner], b[inner] = nu, nc
+        cu, cc = a, b
+    return cu, cc
+
+
 def fused_apply(inputs_by_name: dict, fns, ndim: int, halo_widths, outs=None):
     """Outputs of one fused launch: each member evaluated on the named inputs,
     written into a copy of the corresponding output (zeros if not given)."""

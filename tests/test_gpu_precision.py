@@ -208,3 +208,42 @@ def test_kahan_cuts_small_step_heat_error_against_fp64():
     e32, ek = rel(plain[i32], ref[i64]), rel(comp[ik], ref[i64])
     print(f"heat, {steps} steps: rel L2 vs FP64: fp32 {e32:.3e}, fp32+kahan {ek:.3e}")
     assert ek < 1e-6 and ek * 20 < e32
+
+
+@pytest.mark.parametrize("T", [2, 4])
+def test_kahan_temporal_chain_keeps_compensation_on_chip(T):
+    """T compensated heat steps in one pass: u and its compensation both stay
+    in shared memory between the chained steps (32 B per point per launch,
+    so 32/T per step), bit-exact against T chained oracle Kahan steps; with
+    a zero Dirichlet halo that also equals T separate single-step launches."""
+    import torch
+
+    import cutile
+    from cutile import stencil
+
+    fn = stencil(ndim=2, dtype="float32")(D.heat_small_dt)
+    r = cutile.compile(fn, precision="fp32_kahan", temporal_steps=T)
+    assert r.temporal_steps == T
+    h = r.halo_widths
+    u = D.heat_bump_init(300, halo=h, dtype="float32")
+    c = (np.random.default_rng(9).standard_normal(u.shape) * 1e-9).astype(np.float32)
+    inner = tuple(slice(x, s - x) for x, s in zip(h, u.shape))
+    t = [torch.from_numpy(x).cuda() for x in (u, c)]
+    outs = [torch.full_like(t[0], float("nan")) for _ in range(2)]
+    getattr(r.load_module(), f"launch_{r.name}")(*t, *outs)
+    torch.cuda.synchronize()
+    want_u, want_c = O.kahan_temporal_launch(u, c, _increment_of_heat, 2, h, T)
+    got_u, got_c = (o.cpu().numpy() for o in outs)
+    assert np.array_equal(got_u[inner], want_u[inner])
+    assert np.array_equal(got_c[inner], want_c[inner])
+    # T single-step launches through zero-halo buffers give the same bits
+    r1 = cutile.compile(fn, precision="fp32_kahan", temporal_blocking=False)
+    launch1 = getattr(r1.load_module(), f"launch_{r1.name}")
+    a = [torch.from_numpy(x).cuda() for x in (u, c)]
+    for _ in range(T):
+        b = [torch.zeros_like(a[0]), torch.zeros_like(a[0])]
+        launch1(*a, *b)
+        a = b
+    torch.cuda.synchronize()
+    assert np.array_equal(a[0].cpu().numpy()[inner], got_u[inner])
+    assert np.array_equal(a[1].cpu().numpy()[inner], got_c[inner])

@@ -148,3 +148,29 @@ def test_compile_paths_run_the_verifier(monkeypatch):
     assert len(calls) == 3   # one per fused member
     RKIntegrator(stencil(ndim=2)(D.sw_rhs), "rk2").compile(boundary="reflecting")
     assert len(calls) > 3
+
+
+def test_multi_field_temporal_chains_need_one_output_per_input():
+    """A chain feeds output f into input f of the next step: the compensated
+    (u, c) pair chains; two inputs feeding one output cannot."""
+    import cutile
+    from cutile import stencil
+
+    r = cutile.compile(stencil(ndim=2, dtype="float32")(D.heat_small_dt), precision="fp32_kahan",
+                       temporal_steps=4)
+    assert r.temporal_steps == 4 and r.inputs == ("u", "c_in")
+    with pytest.raises(NotImplementedError, match="one output per input"):
+        cutile.compile(stencil(ndim=2)(D.leapfrog), temporal_steps=2)
+    # without an explicit depth, multi-field stencils keep one step per launch
+    assert cutile.compile(stencil(ndim=2, dtype="float32")(D.heat_small_dt),
+                          precision="fp32_kahan").temporal_steps == 1
+
+
+def test_chain_shared_memory_counts_every_field():
+    from cutile.passes.tiling import EnginePlan, engine_geometry
+
+    p = EnginePlan(2, rows=8, tile_y=1, tile_x=128, vec=4, threads=128, stages=1, zchunk=0,
+                   temporal=4)
+    one = engine_geometry(p, (1, 0, 1), 4, 1)["smem_bytes"]
+    two = engine_geometry(p, (1, 0, 1), 4, 2)["smem_bytes"]
+    assert two > 2 * one - 4096
