@@ -677,28 +677,38 @@ static int build_grid(csd_kernel* k, const csd_field* in, int n_in, const csd_fi
   }
   for (int i = 0; i < n_in; ++i) g->in[i] = in[i].ptr;
   for (int i = 0; i < n_out; ++i) g->out[i] = out[i].ptr;
-  g->xbase = (g->halo[2] / D.align) * D.align;
-  g->tiles[0] = (g->halo[2] + g->interior[2] - g->xbase + D.tile_x - 1) / D.tile_x;
-  g->tiles[1] = (g->interior[1] + D.tile_y - 1) / D.tile_y;
   const long long esz = D.dtype_bytes;
+  long long B = 1;
   if (D.brick_shift > 0) {
     // bricked fields: the shape is the logical (padded-array) shape; bricks
     // of B^ndim elements cover it rounded up to whole bricks
-    const long long B = 1ll << D.brick_shift;
+    B = 1ll << D.brick_shift;
     g->brick_shift = D.brick_shift;
     g->nbx = (int)((g->dims[2] + B - 1) / B);
     g->nby = f0.ndim == 3 ? (int)((g->dims[1] + B - 1) / B) : 1;
-    if (o.loader == CSD_LOADER_TMA)
-      return fail(CSD_EINVAL, "bricked fields are staged with the cp.async loader");
+    if (o.loader == CSD_LOADER_TMA && !D.brick_tma)
+      return fail(CSD_EINVAL, "this bricked kernel stages with the cp.async loader only");
   }
-  // Loader: TMA when every input is 16-byte aligned with 16-byte pitches.
-  bool tma_ok = D.brick_shift == 0 && ((g->pitch_y * esz) % 16 == 0) &&
-                ((g->pitch_z * esz) % 16 == 0);
+  // Loader: TMA when every input is 16-byte aligned with 16-byte pitches
+  // (bricked fields: when the kernel's TMA entry stages bricks).
+  bool tma_ok = D.brick_shift == 0 ? ((g->pitch_y * esz) % 16 == 0) && ((g->pitch_z * esz) % 16 == 0)
+                                   : D.brick_tma != 0;
   for (int i = 0; i < n_in; ++i) tma_ok = tma_ok && (reinterpret_cast<uintptr_t>(in[i].ptr) % 16 == 0);
   int loader = loader_req;
   if (loader < 0 || loader > 1) loader = tma_ok ? CSD_LOADER_TMA : CSD_LOADER_LDG;
   if (loader == CSD_LOADER_TMA && !tma_ok)
     return fail(CSD_EALIGN, "TMA path needs 16-byte aligned fields and row pitch");
+  const bool brick_tma = D.brick_shift > 0 && loader == CSD_LOADER_TMA;
+  // Tile origins: X tiles start at the halo rounded down to 16 bytes (bricked
+  // TMA staging: to a brick), Y tiles at the halo (bricked TMA staging: the
+  // halo rounded down to the tile height, which divides the brick); rows
+  // outside the interior are computed but never stored.  (The tile height
+  // divides the brick or is a multiple of it, so every brick row a tile
+  // covers starts a box.)
+  g->xbase = brick_tma ? (int)((g->halo[2] / B) * B) : (g->halo[2] / D.align) * D.align;
+  g->ybase = brick_tma ? (g->halo[1] / D.tile_y) * D.tile_y : g->halo[1];
+  g->tiles[0] = (g->halo[2] + g->interior[2] - g->xbase + D.tile_x - 1) / D.tile_x;
+  g->tiles[1] = (g->halo[1] + g->interior[1] - g->ybase + D.tile_y - 1) / D.tile_y;
   const long long slots = o.grid > 0 ? o.grid : (long long)k->blocks_per_sm[loader] * st->sms;
   int rc = csd_plan_items(&D, slots, o.zchunk, g);
   if (rc) return rc;
@@ -711,7 +721,35 @@ static int build_grid(csd_kernel* k, const csd_field* in, int n_in, const csd_fi
   for (int i = 0; i < n_out; ++i) vec = vec && (reinterpret_cast<uintptr_t>(out[i].ptr) % 16 == 0);
   if (D.brick_shift == 0) vec = vec && ((g->pitch_y * esz) % 16 == 0) && ((g->pitch_z * esz) % 16 == 0);
   g->vec_store = vec ? 1 : 0;
-  if (loader == CSD_LOADER_TMA) {
+  if (brick_tma) {
+    // 5-D view of a bricked field: (x in brick, brick x, y in brick, z in
+    // brick, brick y + nby * brick z); strides in bytes of dims 1-4.  The
+    // tile map's box is the tile height, the row map's box one row; both
+    // deliver whole-brick rows (box_w / B bricks) as flat rows.
+    Driver& d = drv();
+    const long long nbz = (g->dims[0] + B - 1) / B;
+    const unsigned long long B3 = (unsigned long long)(B * B * B);
+    for (int i = 0; i < n_in; ++i) {
+      unsigned long long gdim[5] = {(unsigned long long)B, (unsigned long long)g->nbx,
+                                    (unsigned long long)B, (unsigned long long)B,
+                                    (unsigned long long)(g->nby * nbz)};
+      unsigned long long gstride[4] = {B3 * esz, (unsigned long long)(B * esz),
+                                       (unsigned long long)(B * B * esz),
+                                       B3 * (unsigned long long)g->nbx * esz};
+      unsigned estride[5] = {1, 1, 1, 1, 1};
+      const unsigned rows = (unsigned)(D.tile_y < B ? D.tile_y : B);  // one brick row at most
+      unsigned box[5] = {(unsigned)B, (unsigned)(D.box_w / B), rows, 1, 1};
+      CUresult r = d.cuTensorMapEncodeTiled(&g->tmap[i], esz == 8 ? TMAP_FLOAT64 : TMAP_FLOAT32, 5,
+                                            const_cast<void*>(in[i].ptr), gdim, gstride, box, estride,
+                                            0, 0, 2, 0);
+      if (r) return cu_fail(r, "cuTensorMapEncodeTiled(bricks)");
+      box[2] = 1;
+      r = d.cuTensorMapEncodeTiled(&g->tmap_wrap[i], esz == 8 ? TMAP_FLOAT64 : TMAP_FLOAT32, 5,
+                                   const_cast<void*>(in[i].ptr), gdim, gstride, box, estride, 0, 0, 2,
+                                   0);
+      if (r) return cu_fail(r, "cuTensorMapEncodeTiled(brick rows)");
+    }
+  } else if (loader == CSD_LOADER_TMA) {
     Driver& d = drv();
     for (int i = 0; i < n_in; ++i) {
       unsigned long long gdim[3] = {(unsigned long long)g->dims[2], (unsigned long long)g->dims[1],

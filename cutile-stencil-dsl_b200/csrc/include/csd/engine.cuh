@@ -65,7 +65,13 @@ struct Cfg {
   typedef T_ T;
   // Bricked layout: BRICK_ = (ndim << 4) | log2(brick size), 0 = flat.
   static constexpr int BRICK_SHIFT = BRICK_ & 15, BRICK_NDIM = BRICK_ >> 4;
-  static_assert(BRICK_ == 0 || LOADER_ == CSD_LOADER_LDG, "bricked fields use the cp.async loader");
+  static constexpr int BRICK_B = BRICK_SHIFT ? (1 << BRICK_SHIFT) : 1;
+  // Bricked fields staged by TMA: a 5-D tensor map over (x in brick, brick
+  // x, y in brick, z in brick, brick y + nby * brick z) turns every box into
+  // flat rows of whole bricks in shared memory, so the chunk layout (and the
+  // body) are those of the flat path; tiles start on a brick in X and on a
+  // tile height that divides the brick in Y.
+  static constexpr bool BTMA = BRICK_SHIFT > 0 && LOADER_ == CSD_LOADER_TMA;
   static constexpr int NIN = NIN_, NOUT = NOUT_;
   static constexpr int RZ = RZ_, RY = RY_, RX = RX_;  // radius of ONE step
   static constexpr int ROWS = ROWS_, TY = TY_, TX = TX_;
@@ -80,9 +86,21 @@ struct Cfg {
   static constexpr int HC = RZ > 0 ? cdiv(RZ, ROWS) : 0;  // halo chunks per side, per step
   // Column layout shared by every buffer: smem column c <-> x = X0 - PADL + c.
   static constexpr int RXA = align_up(RX, ALIGN);
-  static constexpr int PADL = TEMPORAL == 1 ? RXA : align_up(TEMPORAL * RX + 2 * ALIGN - 2, ALIGN);
-  static constexpr int BOXW = TEMPORAL == 1 ? align_up(PADL + TX + RX, ALIGN)
+  // bricked TMA rows: whole bricks, each row 128-byte aligned (TMA destination)
+  static constexpr int BALIGN = imax(BRICK_B, 128 / (int)sizeof(T));
+  static constexpr int PADL = BTMA ? align_up(RX, BRICK_B)
+                            : TEMPORAL == 1 ? RXA : align_up(TEMPORAL * RX + 2 * ALIGN - 2, ALIGN);
+  static constexpr int BOXW = BTMA ? align_up(PADL + TX + RX, BALIGN)
+                            : TEMPORAL == 1 ? align_up(PADL + TX + RX, ALIGN)
                                             : align_up(PADL + TX + TEMPORAL * RX + 2 * ALIGN - 2, ALIGN);
+  static_assert(BRICK_ == 0 || LOADER_ == CSD_LOADER_LDG ||
+                    (BRICK_NDIM == 3 && ROWS_ == 1 && TEMPORAL_ == 1 && BC_ != CSD_BC_PERIODIC &&
+                     (BRICK_B % TY_ == 0 || TY_ % BRICK_B == 0) && TX_ % BRICK_B == 0 &&
+                     (BRICK_B * (int)sizeof(T_)) % 16 == 0 && BOXW / BRICK_B <= 256),
+                "bricked TMA staging: 3-D bricks, one row per chunk, single step, no periodic "
+                "wrap, tile height dividing or divided by the brick, tile width a multiple of it");
+  // rows of one tile-row box (a box stays inside one brick row)
+  static constexpr int BTMA_ROWS = TY_ < BRICK_B ? TY_ : BRICK_B;
   // Height (Y rows) of the buffer holding the field after s steps.
   static __host__ __device__ constexpr int H(int s) { return TY + 2 * (TEMPORAL - s) * RY; }
   static constexpr int BOXH = TY + 2 * TEMPORAL * RY;
@@ -296,7 +314,7 @@ struct Loader {
   // Issue the copies of one chunk (all fields) of grid `g` into `slot`.
   static __device__ __forceinline__ void issue(const csd_grid& g, T* ring, unsigned bar, int slot,
                                                int x0, int y0, int z0) {
-    if constexpr (C::LOADER == CSD_LOADER_TMA) {
+    if constexpr (C::LOADER == CSD_LOADER_TMA && !C::BTMA) {
       if (threadIdx.x == 0) {
         bool left = false, right = false;
         if constexpr (C::PBUF) {
@@ -321,6 +339,39 @@ struct Loader {
             if (right)
               ptx::tma_load_3d(ptx::smem_addr(pbuf + (f * 2 + 1) * C::WRAP_BLOCK),
                                &g.tmap_wrap[f], wrap_x(g, 1), y0, z0, bar);
+          }
+        }
+      }
+    } else if constexpr (C::BTMA) {
+      // Bricked fields, TMA: per field the tile's TY rows in boxes of
+      // BTMA_ROWS rows (one per brick row they cover) and one single-row box
+      // per halo row.  x0 is a multiple of the brick; y0 + RY = Y0 is a
+      // multiple of TY, so every tile-row box lies in one brick row.
+      // Coordinates below zero
+      // or past the bricked extent read zeros; a row just outside the array
+      // in Y may read another brick plane, but such rows only feed points
+      // outside the interior, which are never stored.
+      if (threadIdx.x == 0) {
+        constexpr int S = C::BRICK_SHIFT, BM = C::BRICK_B - 1;
+        ptx::mbar_arrive_expect_tx(bar, (unsigned)(C::CHUNK_BYTES * C::NIN));
+        const int bx = x0 >> S;
+        const int zi = z0 & BM, bz = z0 >> S;
+        const int ym = y0 + C::RY;
+#pragma unroll
+        for (int f = 0; f < C::NIN; ++f) {
+          T* dst = ring + (f * C::NSLOT + slot) * C::SLOT_ELEMS;
+#pragma unroll
+          for (int m = 0; m < C::TY / C::BTMA_ROWS; ++m) {
+            const int y = ym + m * C::BTMA_ROWS;
+            ptx::tma_load_5d(ptx::smem_addr(dst + (C::RY + m * C::BTMA_ROWS) * C::BOXW), &g.tmap[f],
+                             0, bx, y & BM, zi, bz * g.nby + (y >> S), bar);
+          }
+#pragma unroll
+          for (int k = 0; k < 2 * C::RY; ++k) {
+            const int yy = k < C::RY ? k : C::TY + k;   // low halo rows, then high
+            const int y = y0 + yy;
+            ptx::tma_load_5d(ptx::smem_addr(dst + yy * C::BOXW), &g.tmap_wrap[f], 0, bx, y & BM,
+                             zi, bz * g.nby + (y >> S), bar);
           }
         }
       }
@@ -625,7 +676,7 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
     int tx, ty, z0, nrows;
     csd_item_place(&g, item, &tx, &ty, &z0, &nrows);
     const int X0 = g.xbase + tx * C::TX;  // array column of the tile's first point
-    const int Y0 = hy + ty * C::TY;
+    const int Y0 = g.ybase + ty * C::TY;
     const int nsteps = cdiv(nrows, C::ROWS);
     const int nchunks = nsteps + 2 * HCT;
     // array coordinates of input chunk 0

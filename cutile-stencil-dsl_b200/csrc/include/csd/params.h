@@ -6,7 +6,7 @@
 
 #define CSD_MAX_FIELDS 8
 #define CSD_MAX_SCALARS 8
-#define CSD_DESC_MAGIC 0x43534433u /* "CSD3": bumped with every csd_grid layout change */
+#define CSD_DESC_MAGIC 0x43534434u /* "CSD4": bumped with every csd_grid layout change */
 
 #define CSD_LOADER_TMA 0
 #define CSD_LOADER_LDG 1
@@ -68,8 +68,12 @@ typedef struct __attribute__((aligned(64))) csd_grid {
   // brick row-major inside; nbx / nby bricks along X / Y of the padded array.
   int brick_shift;                    // 0: flat (pitched) layout
   int nbx, nby;
+  int ybase;                          // Y origin of tile row 0 (the Y halo, or for bricked
+                                      // TMA staging the halo rounded down to the tile height)
   // Periodic-X kernels (TMA loader): narrow boxes (wrap width x box height x
   // rows) of the inputs, loaded from the far side of a row for X-edge chunks.
+  // Bricked fields staged by TMA: the one-row box of each input (tmap holds
+  // the tile-height box).
   csd_tmap tmap_wrap[CSD_MAX_FIELDS];
 } csd_grid;
 
@@ -141,6 +145,7 @@ typedef struct csd_kernel_desc {
   int ndyn;          // device per-grid scalars the body reads
   int reduce_max;    // 1: the body also max-reduces a value into grid.red
   int brick_shift;   // log2 of the brick size of a bricked-layout kernel (0 = flat)
+  int brick_tma;     // 1: the bricked kernel's TMA entry stages bricks with tensor copies
 } csd_kernel_desc;
 
 #ifdef __cplusplus

@@ -75,6 +75,18 @@ __device__ __forceinline__ void tma_load_3d(unsigned dst, const void* tmap, int 
       : "memory");
 }
 
+// 5-D TMA tile load into shared memory (bricked fields: x in brick, brick x,
+// y in brick, z in brick, brick y/z), completion counted on `bar`.
+__device__ __forceinline__ void tma_load_5d(unsigned dst, const void* tmap, int c0, int c1, int c2,
+                                            int c3, int c4, unsigned bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(dst),
+      "l"(reinterpret_cast<unsigned long long>(tmap)), "r"(c0), "r"(c1), "r"(c2), "r"(c3),
+      "r"(c4), "r"(bar)
+      : "memory");
+}
+
 // Element copy global->shared with zero fill when `valid` is false.
 template <int BYTES>
 __device__ __forceinline__ void cp_async_zfill(unsigned dst, const void* src, bool valid) {

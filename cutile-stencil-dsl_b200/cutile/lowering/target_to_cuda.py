@@ -357,6 +357,25 @@ def engine_params(kernel: KernelOp) -> dict:
     }
 
 
+def brick_tma_eligible(p: dict) -> bool:
+    """Whether a bricked kernel's TMA entry can stage bricks with tensor copies
+    (engine.cuh ``Cfg::BTMA``): 3-D bricks, one Z row per chunk, one step, no
+    periodic wrap, a tile height dividing the brick or a multiple of it and
+    a tile width that is a whole number of bricks, bricks at least 16 bytes wide, at most 256
+    bricks per staged row."""
+    code = p["BRICK"]
+    if not code or (code >> 4) != 3:
+        return False
+    b = 1 << (code & 15)
+    esz = p["dtype_bytes"]
+    balign = max(b, 128 // esz)
+    padl = -(-p["RX"] // b) * b
+    boxw = -(-(padl + p["TX"] + p["RX"]) // balign) * balign
+    return (p["ROWS"] == 1 and p["TEMPORAL"] == 1 and p["BC"] != BC_CODES["periodic"]
+            and (b % p["TY"] == 0 or p["TY"] % b == 0) and p["TX"] % b == 0 and (b * esz) % 16 == 0
+            and boxw // b <= 256)
+
+
 def _brick_code(kernel: KernelOp, ndim: int) -> int:
     """(ndim << 4) | log2(brick size) for a bricked-layout kernel, else 0."""
     if kernel.layout is None or kernel.layout.data != "bricked":
@@ -391,9 +410,10 @@ def emit_cuda(module: ModuleOp, preamble: bool = True) -> str:
         parts.append(f"// expression: {kernel.expression.data}")
         parts.append(emit_body(kernel))
         parts.append("")
+        brick_tma = brick_tma_eligible(p)
         for suffix, loader in (("tma", "CSD_LOADER_TMA"), ("ldg", "CSD_LOADER_LDG")):
-            if p["BRICK"]:
-                loader = "CSD_LOADER_LDG"   # bricked fields: both entries use cp.async
+            if p["BRICK"] and not brick_tma:
+                loader = "CSD_LOADER_LDG"   # bricked fields the TMA boxes cannot stage
             cfg = (f"csd::Cfg<{p['T']}, {p['NIN']}, {p['NOUT']}, {p['RZ']}, {p['RY']}, {p['RX']}, "
                    f"{p['ROWS']}, {p['TY']}, {p['TX']}, {p['NT']}, {p['STAGES']}, {p['TEMPORAL']}, "
                    f"{loader}, {p['BC']}, {p['REDUCE']}, {p['BRICK']}, {p['RPY']}>")
@@ -408,11 +428,15 @@ def emit_cuda(module: ModuleOp, preamble: bool = True) -> str:
         parts.append(f"  CSD_DESC_MAGIC, {p['ndim']}, {c}::NIN, {nout_desc}, (int)sizeof({c}::T),")
         parts.append(f"  {c}::RZ * {c}::TEMPORAL, {c}::RY * {c}::TEMPORAL, {c}::RX * {c}::TEMPORAL,")
         parts.append(f"  {c}::ROWS, {c}::TY, {c}::TX, {c}::VEC, {c}::NT, {c}::STAGES, {c}::NSLOT,")
-        parts.append(f"  {c}::HC * {c}::TEMPORAL, {c}::PADL, {c}::BOXW, {c}::BOXH, {c}::SMEM_BYTES,")
+        # both entries launch with one shared-memory size: the larger one
+        smem = (f"({c}::SMEM_BYTES > Cfg_{name}_ldg::SMEM_BYTES ? {c}::SMEM_BYTES : "
+                f"Cfg_{name}_ldg::SMEM_BYTES)")
+        parts.append(f"  {c}::HC * {c}::TEMPORAL, {c}::PADL, {c}::BOXW, {c}::BOXH, {smem},")
         parts.append(f"  {p['ZCHUNK']}, {c}::TEMPORAL, {c}::BC, {p['MINB']}, {c}::ALIGN,")
-        parts.append(f"  {p['NSCAL']}, {p['NDYN']}, {p['REDUCE']}, {c}::BRICK_SHIFT}};")
+        parts.append(f"  {p['NSCAL']}, {p['NDYN']}, {p['REDUCE']}, {c}::BRICK_SHIFT, "
+                     f"{1 if brick_tma else 0}}};")
         parts.append("")
     return "\n".join(parts) + "\n"
 
 
-__all__ = ["emit_cuda", "emit_body", "engine_params", "hex_literal"]
+__all__ = ["emit_cuda", "emit_body", "engine_params", "hex_literal", "brick_tma_eligible"]

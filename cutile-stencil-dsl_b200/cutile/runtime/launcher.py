@@ -542,8 +542,12 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
         # (stencil_to_target.py:796-800), so a multi-field stencil cannot run
         # blocked there either; it advances one step per launch.
         T = 1
-    plan = _plan_from(tile_sizes, kernel_hints, len(stencil_halo),
-                      replace(plan, temporal=T, rpy=plan.rpy if T == 1 else 1))
+    plan = replace(plan, temporal=T, rpy=plan.rpy if T == 1 else 1)
+    if layout == "bricked" and len(stencil_halo) == 3 and tile_sizes is None:
+        # one Z row per chunk, so that the bricked kernel can stage bricks
+        # with tensor copies (target_to_cuda.brick_tma_eligible)
+        plan = replace(plan, rows=1)
+    plan = _plan_from(tile_sizes, kernel_hints, len(stencil_halo), plan)
     if occupancy is not None:
         plan = replace(plan, occupancy=int(occupancy))
     plan = fit_plan(plan, stencil_halo, dtype_bytes, num_inputs, analysis.get("body_ops", 0))

@@ -190,10 +190,11 @@ class StencilProgram:
         return native.from_bricks(bricked, shape, int(brick_size), stream=stream)
 
     def launch_on_bricks(self, inputs, outputs, shape, stream=None, *,
-                         scalars: dict | None = None) -> None:
+                         scalars: dict | None = None, loader: int = -1) -> None:
         """The bricked kernel on bricked fields of a ``shape`` array: writes
         the interior cells of the outputs' bricks (halo and padding cells
-        untouched)."""
+        untouched).  ``loader``: -1 picks TMA brick staging where the kernel
+        has it, else per-group cp.async copies."""
         bs = self._brick(self.spec["brick_size"])
         shape = tuple(int(n) for n in shape)
         if len(shape) != self.spec["ndim"]:
@@ -213,7 +214,7 @@ class StencilProgram:
         fin = [native.bricked_field(t, shape, bs) for t in inputs]
         fout = [native.bricked_field(t, shape, bs) for t in outputs]
         native.launch_fields(self.kernel("bricked"), fin, fout, self.spec["halo"], stream,
-                             loader=native.CSD_LOADER_LDG, scalars=self.scalar_values(scalars))
+                             loader=loader, scalars=self.scalar_values(scalars))
 
     def launch_bricked(self, inputs, outputs, brick_size, stream=None, *,
                        scalars: dict | None = None) -> None:

@@ -67,7 +67,7 @@ class KernelDesc(ctypes.Structure):
         "magic", "ndim", "nin", "nout", "dtype_bytes", "rz", "ry", "rx", "rows", "tile_y",
         "tile_x", "vec", "threads", "stages", "nslot", "halo_chunks", "pad_left", "box_w",
         "box_h", "smem_bytes", "zchunk", "temporal", "bc_mode", "min_blocks", "align",
-        "nscalars", "ndyn", "reduce_max", "brick_shift")]
+        "nscalars", "ndyn", "reduce_max", "brick_shift", "brick_tma")]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}

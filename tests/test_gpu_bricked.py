@@ -81,3 +81,70 @@ def test_resident_bricks_equal_flat_kernel(ndim):
     halo_mask = np.ones(shape, bool)
     halo_mask[inner] = False
     assert (got[halo_mask] == 7.0).all()
+
+
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+@pytest.mark.parametrize("b", [4, 8, 16])
+@pytest.mark.parametrize("shape", [(18, 18, 34), (21, 19, 45), (9, 40, 70)])
+def test_bricked_tma_staging_equals_cp_async_and_flat(dtype, b, shape):
+    """Bricks staged by 5-D tensor copies (whole-brick rows, tiles on brick
+    boundaries) give the bits of the per-group cp.async staging and of the
+    flat kernel, on shapes that are not whole bricks."""
+    import torch
+
+    from cutile import compile as stencil_compile
+    from cutile import stencil
+    from cutile.runtime import native
+
+    r = stencil_compile(stencil(ndim=3, dtype=dtype)(D.lap7), layout="bricked", brick_size=b,
+                        temporal_blocking=False)
+    mod = r.load_module()
+    prog = mod.program()
+    assert prog.kernel("bricked").desc["brick_tma"] == 1
+    u = np.random.default_rng(sum(shape) + b).random(shape).astype(dtype)
+    a = torch.from_numpy(u).cuda()
+    flat_out = torch.zeros_like(a)
+    getattr(mod, f"launch_{r.name}")(a, flat_out)
+    ab = mod.to_bricks(a)
+    outs = []
+    for loader in (native.CSD_LOADER_TMA, native.CSD_LOADER_LDG):
+        ob = torch.full_like(ab, 7.0)
+        prog.launch_on_bricks((ab,), (ob,), shape, loader=loader)
+        outs.append(mod.from_bricks(ob, shape).cpu().numpy())
+    torch.cuda.synchronize()
+    inner = tuple(slice(1, s - 1) for s in shape)
+    assert np.array_equal(outs[0], outs[1])
+    assert np.array_equal(outs[0][inner], flat_out.cpu().numpy()[inner])
+    want = O.apply_stencil(u, D.lap7, 3, (1, 1, 1))
+    assert np.array_equal(outs[0][inner], want[inner])
+    halo_mask = np.ones(shape, bool)
+    halo_mask[inner] = False
+    assert (outs[0][halo_mask] == 7.0).all()
+    assert native.error_word(reset=True) == 0
+
+
+def test_bricked_box27_tma_staging():
+    """A 27-point box (corner reads across brick rows) on TMA-staged bricks."""
+    import tempfile
+
+    import torch
+
+    import ref_corpus as RC
+    from cutile import compile as stencil_compile
+    from cutile.runtime import native
+
+    entries, _ = RC.load()
+    with tempfile.TemporaryDirectory() as tmp:
+        fn = RC.build(tmp, "wide_stencils/box27", entries["wide_stencils/box27"])
+    r = stencil_compile(fn, layout="bricked", brick_size=8, temporal_blocking=False)
+    mod = r.load_module()
+    shape = (20, 27, 53)
+    u = np.random.default_rng(5).random(shape)
+    ab = mod.to_bricks(torch.from_numpy(u).cuda())
+    ob = torch.zeros_like(ab)
+    getattr(mod, f"launch_{r.name}_on_bricks")(ab, ob, shape)
+    got = mod.from_bricks(ob, shape).cpu().numpy()
+    want = O.apply_stencil(u, fn, 3, (1, 1, 1))
+    inner = tuple(slice(1, s - 1) for s in shape)
+    assert np.array_equal(got[inner], want[inner])
+    assert native.error_word(reset=True) == 0
