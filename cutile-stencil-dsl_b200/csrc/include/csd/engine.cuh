@@ -841,16 +841,22 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
               }
             } else {
               // intermediate field(s): zero outside the domain interior, as
-              // the zero-halo scratch buffers of T separate launches hold
+              // the zero-halo scratch buffers of T separate launches hold;
+              // a unit wholly inside stores one 16-byte vector per field
+              const bool whole = zin && yin && gx0 >= hx && gx0 + C::VEC <= hx + nx;
 #pragma unroll
               for (int f = 0; f < C::NOUT; ++f) {
                 T* d = dst + f * C::NSLOT_I * C::ISLOT_ELEMS(s) + (r * hs + y + j) * C::BOXW +
                        xv * C::VEC;
+                if (whole) {
+                  store_vec(d, ov[f]);
+                } else {
 #pragma unroll
-                for (int e = 0; e < C::VEC; ++e) {
-                  const int gx = gx0 + e;
-                  const bool in = zin && yin && gx >= hx && gx < hx + nx;
-                  d[e] = in ? ov[f][e] : T(0);
+                  for (int e = 0; e < C::VEC; ++e) {
+                    const int gx = gx0 + e;
+                    const bool in = zin && yin && gx >= hx && gx < hx + nx;
+                    d[e] = in ? ov[f][e] : T(0);
+                  }
                 }
               }
             }
