@@ -105,7 +105,12 @@ struct Cfg {
   static __host__ __device__ constexpr int H(int s) { return TY + 2 * (TEMPORAL - s) * RY; }
   static constexpr int BOXH = TY + 2 * TEMPORAL * RY;
   static constexpr int NSLOT = 2 * HC + 1 + STAGES;              // input ring
-  static constexpr int NSLOT_I = 2 * HC + 1;                     // intermediate rings
+  // Intermediate rings: stage s + 1 reads field s only from chunks finished
+  // in earlier ring steps, so one slot more than the 2*HC+1 it reads is being
+  // written meanwhile (one barrier per ring step, not one per stage).
+  static constexpr int NSLOT_I = 2 * HC + 2;
+  // Chunk of field s computed at ring step i: i - STAGE_OFF(s).
+  static __host__ __device__ constexpr int STAGE_OFF(int s) { return s * HC + (s - 1); }
   static constexpr int SLOT_ELEMS = align_up(ROWS * BOXH * BOXW, 128 / (int)sizeof(T));
   static constexpr int CHUNK_BYTES = ROWS * BOXH * BOXW * (int)sizeof(T);  // TMA bytes
   static __host__ __device__ constexpr int ISLOT_ELEMS(int s) {
@@ -707,9 +712,10 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
         Loader<C>::issue(g, ring, ptx::smem_addr(&bars[slot]), slot, cx, cy, cz + k * C::ROWS);
     }
 
-    for (int i = 0; i < nchunks; ++i) {
+    // ring steps: one per input chunk, then T-1 more that drain the chain
+    for (int i = 0; i < nchunks + T_ - 1; ++i) {
       // wait for input chunk i
-      {
+      if (i < nchunks) {
         const unsigned gq = seq + i;
         const int slot = gq % C::NSLOT;
         const unsigned parity = (gq / C::NSLOT) & 1u;
@@ -730,10 +736,14 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
       __syncthreads();
       if (abort_flag) break;
 
-      // stages 1..T: stage s computes chunk k_s = i - s*HC of its field
+      // stages 1..T: stage s computes chunk k_s = i - STAGE_OFF(s) of its
+      // field; stage 1 reads input chunks up to i (landed above), stage
+      // s > 1 reads field s-1 up to chunk k_s + HC = i - STAGE_OFF(s-1) - 1,
+      // finished at an earlier step, so the stages need no barrier between
+      // them
 #pragma unroll
       for (int s = 1; s <= T_; ++s) {
-        const int k = i - s * C::HC;   // chunk index in the common chunk grid
+        const int k = i - C::STAGE_OFF(s);   // chunk index in the common chunk grid
         const int klo = s * C::HC;     // first chunk of field s that is needed
         const int khi = nsteps + (2 * T_ - s) * C::HC;  // one past the last
         if (k < klo || k >= khi) continue;
@@ -873,8 +883,10 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
 #pragma unroll 1
           for (int u = threadIdx.x; u < units; u += C::NT) unit(u);
         }
-        __syncthreads();
       }
+      // every stage's reads of this step are done before the refill below
+      // and before the next step overwrites a ring slot
+      __syncthreads();
 
       // refill: input chunk i - 2*HC is dead, its slot takes chunk i - 2*HC + NSLOT
       {
