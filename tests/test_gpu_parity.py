@@ -164,8 +164,9 @@ def test_heat_1024_100_steps_ping_pong():
 
 
 @pytest.mark.parametrize("name,ndim,T", [("heat2d", 2, None), ("heat1d", 1, None),
-                                          ("lap7", 3, 2), ("lap7", 3, 3), ("heat2d", 2, 4),
-                                          ("lap4_1d", 1, 3), ("wave4", 2, 2)])
+                                          ("lap7", 3, 2), ("lap7", 3, 3), ("lap7", 3, 4),
+                                          ("lap7", 3, 8), ("heat2d", 2, 4), ("heat2d", 2, 8),
+                                          ("lap4_1d", 1, 3), ("wave4", 2, 2), ("wave4", 2, 4)])
 def test_temporal_blocking_matches_T_launches(name, ndim, T):
     import cutile
 
