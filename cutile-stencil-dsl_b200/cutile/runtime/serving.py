@@ -126,6 +126,7 @@ class StencilServer:
         self.device = torch.device(device)
         self._progs: dict = {}
         self._idx_bufs: dict = {}
+        self._host_bufs: dict = {}  # pinned staging of the index lists, per group and parity
         self._pool = None          # device descriptors of every active solve, all phases
         self._pool_top = 0
         self._pool_free: dict = {}  # phases -> free slot blocks
@@ -252,16 +253,24 @@ class StencilServer:
         for key, members in groups.items():
             prog, kern, zc = self.program(*key)
             n = len(members)
-            host = np.empty(2 * n + 1, dtype=np.int32)
+            size = 2 * n + 1
+            # pinned staging buffers alternate like the device ones: the copy
+            # that read a buffer two iterations ago has finished
+            hbufs = self._host_bufs.setdefault(key, [None, None])
+            hb = hbufs[parity]
+            if hb is None or hb.numel() < size:
+                hb = torch.empty(max(2 * size, 1024), dtype=torch.int32, pin_memory=True)
+                hbufs[parity] = hb
+            host = hb.numpy()[:size]
             host[:n] = [a.slot + a.phase for a in members]
             host[n] = 0
             np.cumsum([a.items for a in members], out=host[n + 1:])
             bufs = self._idx_bufs.setdefault(key, [None, None])
             buf = bufs[parity]
-            if buf is None or buf.numel() < host.size:
-                buf = torch.empty(max(2 * host.size, 1024), dtype=torch.int32, device=self.device)
+            if buf is None or buf.numel() < size:
+                buf = torch.empty(max(2 * size, 1024), dtype=torch.int32, device=self.device)
                 bufs[parity] = buf
-            buf[:host.size].copy_(torch.from_numpy(host).pin_memory(), non_blocking=True)
+            buf[:size].copy_(hb[:size], non_blocking=True)
             native.launch_batch(kern, self._pool.data_ptr(), buf.data_ptr() + 4 * n, n,
                                 int(host[-1]), stream, loader=native.CSD_LOADER_TMA,
                                 grid_index_ptr=buf.data_ptr())
