@@ -30,11 +30,13 @@ namespace csd {
 
 // Bound on the drain of an aborted work item (copies still in flight).
 constexpr unsigned long long kDrainNs = 2000000000ull;
-// Stages with at most this many units per thread unroll their unit loop.
-#ifndef CSD_UNROLL_UNITS
-#define CSD_UNROLL_UNITS 4
+// Temporal chains: with CSD_CHAIN_SKEW (the default) stage s + 1 reads
+// field s only from chunks finished at earlier ring steps (one more ring slot
+// per stage, one barrier per ring step); without it stage s + 1 reads the
+// chunk stage s wrote in the same step (a barrier after every stage).
+#ifndef CSD_CHAIN_SKEW
+#define CSD_CHAIN_SKEW 1
 #endif
-constexpr int kUnrollUnits = CSD_UNROLL_UNITS;
 
 template <typename T>
 struct VecOf;
@@ -108,9 +110,10 @@ struct Cfg {
   // Intermediate rings: stage s + 1 reads field s only from chunks finished
   // in earlier ring steps, so one slot more than the 2*HC+1 it reads is being
   // written meanwhile (one barrier per ring step, not one per stage).
-  static constexpr int NSLOT_I = 2 * HC + 2;
+  static constexpr bool SKEW = CSD_CHAIN_SKEW != 0;
+  static constexpr int NSLOT_I = 2 * HC + (SKEW ? 2 : 1);
   // Chunk of field s computed at ring step i: i - STAGE_OFF(s).
-  static __host__ __device__ constexpr int STAGE_OFF(int s) { return s * HC + (s - 1); }
+  static __host__ __device__ constexpr int STAGE_OFF(int s) { return s * HC + (SKEW ? s - 1 : 0); }
   static constexpr int SLOT_ELEMS = align_up(ROWS * BOXH * BOXW, 128 / (int)sizeof(T));
   static constexpr int CHUNK_BYTES = ROWS * BOXH * BOXW * (int)sizeof(T);  // TMA bytes
   static __host__ __device__ constexpr int ISLOT_ELEMS(int s) {
@@ -670,6 +673,13 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
   typedef typename C::T T;
   constexpr int T_ = C::TEMPORAL;
   constexpr int HCT = C::HC * T_;  // input halo chunks per side for the whole chain
+  // units per thread up to which a stage unrolls its unit loop (the body's
+  // choice: small bodies gain, wide ones would keep several units' strips live)
+#ifdef CSD_UNROLL_UNITS
+  constexpr int UNR = CSD_UNROLL_UNITS;
+#else
+  constexpr int UNR = Body::UNROLL;
+#endif
   unsigned seq = 0;                // chunks consumed by this CTA so far
   const int total = BATCHED ? p.total_items : p.g.items;
 
@@ -713,7 +723,7 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
     }
 
     // ring steps: one per input chunk, then T-1 more that drain the chain
-    for (int i = 0; i < nchunks + T_ - 1; ++i) {
+    for (int i = 0; i < nchunks + (C::SKEW ? T_ - 1 : 0); ++i) {
       // wait for input chunk i
       if (i < nchunks) {
         const unsigned gq = seq + i;
@@ -875,13 +885,16 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
         // A short, exact count of units per thread is unrolled, so that the
         // units' coordinates fold into per-thread constants; longer or
         // ragged counts loop.
-        if (units % C::NT == 0 && units / C::NT <= kUnrollUnits) {
+        if (units % C::NT == 0 && units / C::NT <= UNR) {
 #pragma unroll
-          for (int q = 0; q < kUnrollUnits; ++q)
+          for (int q = 0; q < (UNR > 0 ? UNR : 1); ++q)
             if (q < units / C::NT) unit(threadIdx.x + q * C::NT);
         } else {
 #pragma unroll 1
           for (int u = threadIdx.x; u < units; u += C::NT) unit(u);
+        }
+        if constexpr (!C::SKEW) {
+          if (s < T_) __syncthreads();   // stage s + 1 reads what stage s just wrote
         }
       }
       // every stage's reads of this step are done before the refill below

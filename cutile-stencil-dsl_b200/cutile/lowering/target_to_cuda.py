@@ -209,7 +209,13 @@ def emit_body(kernel: KernelOp) -> str:
             groups.setdefault((f, dz, dy + j), []).append(dx)
     gkeys = list(groups)
     gindex = {key: gi for gi, key in enumerate(gkeys)}
+    # small bodies let the engine unroll a stage's units (their coordinates
+    # fold into per-thread constants); wide ones would keep several units'
+    # strips live at once and spill
+    body_lines = sum(len(prog.data) for prog in kernel.ssa_body.data)
+    unroll = 4 if (len(gkeys) <= 8 and rpy == 1 and body_lines <= 48) else 0
     out = [f"struct Body_{name} {{",
+           f"  static constexpr int UNROLL = {unroll};",
            "  template <class C>",
            "  __device__ __forceinline__ static void compute(const csd::TileView<C>& t, int r, int y,",
            "                                                 int x, csd::OutPack<typename C::T, "

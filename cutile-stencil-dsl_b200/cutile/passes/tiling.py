@@ -202,7 +202,7 @@ def engine_geometry(plan: EnginePlan, radius3: tuple[int, int, int], dtype_bytes
         box_w = _align_up(pad_left + plan.tile_x + T * rx + 2 * align - 2, align)
     box_h = plan.tile_y + 2 * T * ry
     nslot = 2 * hc + 1 + plan.stages
-    nslot_i = 2 * hc + 2   # engine.cuh Cfg::NSLOT_I
+    nslot_i = 2 * hc + 2   # engine.cuh Cfg::NSLOT_I (chain skew on)
     per128 = 128 // dtype_bytes
     slot_elems = _align_up(plan.rows * box_h * box_w, per128)
     inter = num_inputs * sum(nslot_i * _align_up(plan.rows * (plan.tile_y + 2 * (T - s) * ry) * box_w,

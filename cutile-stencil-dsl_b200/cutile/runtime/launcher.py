@@ -445,6 +445,30 @@ def generate_module_code(name: str, cuda_source: str, spec: dict, *, fused_outpu
     return e.render()
 
 
+def _rpy_keeps_registers(stencil_fn, plan, stencil_halo, halo_widths, dtype, dtype_bytes,
+                         num_inputs, T, body_ops, kahan) -> bool:
+    """Whether the rows-per-thread default compiles without spills for this
+    body.  Dense boxes whose terms the DSL orders irregularly keep many strips
+    live at once; ptxas' report of the NVRTC build (cached, so the module
+    load reuses it) decides.  Without a working NVRTC the plan is kept."""
+    from cutile.lowering.stencil_to_target import lower_to_target_ir
+    from cutile.lowering.target_to_cuda import emit_cuda
+    from cutile.passes.tiling import fit_plan
+    from cutile.runtime import native
+    from cutile.runtime.regcheck import parse_ptxas_log
+
+    p = fit_plan(plan, stencil_halo, dtype_bytes, num_inputs, body_ops)
+    target = lower_to_target_ir(stencil_fn._ir.clone(), p.tile_sizes(), halo_widths,
+                                temporal_steps=T, kernel_hints=p.hints(), dtype=dtype,
+                                kahan=kahan)
+    try:
+        _, log = native.compile_source(emit_cuda(target))
+    except Exception:  # noqa: BLE001 - no NVRTC here: keep the measured default
+        return True
+    res = parse_ptxas_log(log, f"{stencil_fn._fn.__name__}_tma")
+    return res is None or not res.spills
+
+
 def _analysis_of(clone) -> tuple:
     halo_widths, tile_sizes, temporal_steps = (1,), (256,), 1
     analysis, occupancy, num_loads = {}, None, 0
@@ -543,6 +567,13 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
         # blocked there either; it advances one step per launch.
         T = 1
     plan = replace(plan, temporal=T, rpy=plan.rpy if T == 1 else 1)
+    hinted_rpy = bool(kernel_hints) and ("rows_per_thread" in kernel_hints or "rpy" in kernel_hints)
+    if plan.rpy > 1 and tile_sizes is None and not hinted_rpy and not _rpy_keeps_registers(
+            stencil_fn, plan, stencil_halo, halo_widths, dtype, dtype_bytes, num_inputs, T,
+            analysis.get("body_ops", 0), kahan):
+        # the default rows-per-thread plan would spill this body's strips:
+        # one row per thread over the wide tile instead
+        plan = replace(plan, rpy=1, rows=1, tile_y=4, tile_x=64)
     if layout == "bricked" and len(stencil_halo) == 3 and tile_sizes is None:
         # one Z row per chunk, so that the bricked kernel can stage bricks
         # with tensor copies (target_to_cuda.brick_tma_eligible)

@@ -496,3 +496,22 @@ def test_tuple_returning_stencil_keeps_one_row_per_thread():
         spec.loader.exec_module(m)
         r = cutile.compile(m.two, temporal_blocking=False, autotune=False)
     assert "rpy" not in r.kernel_hints
+
+
+def test_rows_per_thread_default_falls_back_when_it_would_spill():
+    """The reference's box125 (46 irregularly ordered terms) spills at two
+    rows per thread, so its default plan keeps one row; the regular 125-point
+    box keeps the two-row plan."""
+    import tempfile
+
+    import cutile
+    import ref_corpus as RC
+    import wide_defs as W
+
+    entries, _ = RC.load()
+    with tempfile.TemporaryDirectory() as tmp:
+        fn = RC.build(tmp, "wide_stencils/box125", entries["wide_stencils/box125"])
+        r = cutile.compile(fn, temporal_blocking=False)
+    assert "rpy" not in r.kernel_hints
+    r2 = cutile.compile(W.load_box("regular_box125", 2), temporal_blocking=False)
+    assert r2.kernel_hints.get("rpy") == 2
