@@ -190,7 +190,7 @@ class StencilProgram:
         return native.from_bricks(bricked, shape, int(brick_size), stream=stream)
 
     def launch_on_bricks(self, inputs, outputs, shape, stream=None, *,
-                         scalars: dict | None = None, loader: int = -1) -> None:
+                         scalars: dict | None = None, loader: int = -1, zchunk: int = 0) -> None:
         """The bricked kernel on bricked fields of a ``shape`` array: writes
         the interior cells of the outputs' bricks (halo and padding cells
         untouched).  ``loader``: -1 picks TMA brick staging where the kernel
@@ -214,7 +214,7 @@ class StencilProgram:
         fin = [native.bricked_field(t, shape, bs) for t in inputs]
         fout = [native.bricked_field(t, shape, bs) for t in outputs]
         native.launch_fields(self.kernel("bricked"), fin, fout, self.spec["halo"], stream,
-                             loader=loader, scalars=self.scalar_values(scalars))
+                             loader=loader, zchunk=zchunk, scalars=self.scalar_values(scalars))
 
     def launch_bricked(self, inputs, outputs, brick_size, stream=None, *,
                        scalars: dict | None = None) -> None:
