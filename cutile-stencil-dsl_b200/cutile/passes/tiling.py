@@ -320,7 +320,9 @@ def fit_plan(plan: EnginePlan, radius: tuple[int, ...], dtype_bytes: int,
     # several shorter items per resident block so that blocks finish together
     # (measured on B200, 2-D shallow water RK stage on 2048^2: 16-row items
     # 114 us vs one 128-row item per block 184 us).
-    waves = plan.waves if plan.waves > 0 else (8 if body_ops > 60 else 1)
+    # Temporal chains are latency-bound the same way (measured on 512^3 FP64,
+    # T=2, 8 x 64 tiles: one wave 308, eight waves 343 GPts/s).
+    waves = plan.waves if plan.waves > 0 else (8 if body_ops > 60 or plan.temporal > 1 else 1)
     return replace(plan, threads=threads, zchunk=zchunk, min_blocks=min_blocks, waves=waves)
 
 

@@ -73,3 +73,33 @@ def test_boundary_split_shortens_edge_items_within_one_wave():
     assert edge <= 0.8 * mid
     inner = sorted(cover[(5, 0)])
     assert inner[0][1] < inner[1][1] and inner[-1][1] < inner[1][1]
+
+
+def test_single_wave_kept_when_it_fills_the_slots():
+    """512 columns on 1184 resident slots (the flat 7-point sweep at 512^3):
+    two items per column, one wave, 86 % of the slots busy."""
+    split, items = _plan(CSD_BC_NONE, 1, 4, 128, 512, 1184)
+    assert split["items"] == 1024 <= 1184
+
+
+@pytest.mark.parametrize("tx,ty,slots", [(5, 129, 1184), (4, 128, 444), (3, 80, 444)])
+def test_poorly_filled_single_wave_becomes_about_seven_waves(tx, ty, slots):
+    """Columns that would leave more than a fifth of the slots idle (the
+    bricked sweep's 645 columns on 1184 slots; 512 columns on 444 slots,
+    which spill into a thin second wave) are cut into shorter items, about
+    seven waves, every row still written once."""
+    split, items = _plan(CSD_BC_NONE, 1, tx, ty, 512, slots)
+    waves = split["items"] / slots
+    assert 5.5 <= waves <= 8.5, waves
+    _coverage(items, tx, ty, 512)
+
+
+def test_chains_default_to_eight_waves():
+    from cutile.passes.tiling import EnginePlan, fit_plan
+
+    p = fit_plan(EnginePlan(3, rows=1, tile_y=8, tile_x=64, vec=2, threads=128, stages=1,
+                            zchunk=0, temporal=2), (1, 1, 1), 8, 1)
+    assert p.waves == 8
+    p1 = fit_plan(EnginePlan(3, rows=1, tile_y=4, tile_x=128, vec=2, threads=128, stages=1,
+                             zchunk=0), (1, 1, 1), 8, 1)
+    assert p1.waves == 1
