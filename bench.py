@@ -269,7 +269,7 @@ def run_ours(args) -> dict:
     e2e_gpts = npts * T * sweeps / (e2e_ms / 1e3) / 1e9 * world
     a, b = pairs[0]
 
-    traffic = _profiled_traffic(args.dtype, T)
+    traffic = _profiled_traffic(args.dtype, T, args.layout)
     cpu = cpu_baseline(np_dtype) if (rank == 0 and world == 1 and not args.no_cpu) else None
     line = {
         "metric": METRIC, "value": round(gpts, 3), "unit": "GPts/s", "n_gpus": world,
@@ -301,14 +301,14 @@ def run_ours(args) -> dict:
     return line if rank == 0 else None
 
 
-def _profiled_traffic(dtype: str, T: int):
+def _profiled_traffic(dtype: str, T: int, layout: str = "flat"):
     """DRAM bytes per launch from the committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", "lap7_512_traffic.json")
     if not os.path.exists(path):
         return None
     with open(path) as f:
         d = json.load(f)
-    return d.get(f"{dtype}_T{T}")
+    return d.get(f"{dtype}_T{T}" + ("_bricked" if layout == "bricked" else ""))
 
 
 def _slab_job(args):
