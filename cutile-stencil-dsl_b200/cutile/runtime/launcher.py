@@ -580,6 +580,12 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
         # whose larger rings leave 3 blocks per SM and 512 columns for 444
         # resident slots)
         plan = replace(plan, rows=1, tile_y=8, tile_x=64, threads=128)
+    elif T > 1 and len(stencil_halo) == 2 and tile_sizes is None:
+        # 2-D chains (measured on heat 4096^2 FP64): T=2 over 8 x 64 chunks,
+        # 128 threads, 346 GPts/s (8 x 128: 317); deeper chains over 4 x 128
+        # chunks, 256 threads, T=4 256 (8 x 128: 161, one block per SM)
+        plan = (replace(plan, rows=8, tile_x=64, threads=128) if T == 2 else
+                replace(plan, rows=4, tile_x=128, threads=256))
     if layout == "bricked" and len(stencil_halo) == 3 and tile_sizes is None:
         # one Z row per chunk, so that the bricked kernel can stage bricks
         # with tensor copies (target_to_cuda.brick_tma_eligible)
