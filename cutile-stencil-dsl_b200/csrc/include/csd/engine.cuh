@@ -37,6 +37,10 @@ constexpr unsigned long long kDrainNs = 2000000000ull;
 #ifndef CSD_CHAIN_SKEW
 #define CSD_CHAIN_SKEW 1
 #endif
+// Unroll also unit counts that do not divide the block (last round predicated).
+#ifndef CSD_UNROLL_RAGGED
+#define CSD_UNROLL_RAGGED 1
+#endif
 
 template <typename T>
 struct VecOf;
@@ -882,13 +886,16 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
             }
           }  // rows of the unit
         };
-        // A short, exact count of units per thread is unrolled, so that the
-        // units' coordinates fold into per-thread constants; longer or
-        // ragged counts loop.
-        if (units % C::NT == 0 && units / C::NT <= UNR) {
+        // A short count of units per thread is unrolled, so that the units'
+        // coordinates fold into per-thread constants and their loads overlap;
+        // longer counts loop.
+        if ((units % C::NT == 0 || CSD_UNROLL_RAGGED) && cdiv(units, C::NT) <= UNR) {
+          // a ragged last round is predicated off for the threads past the end
 #pragma unroll
-          for (int q = 0; q < (UNR > 0 ? UNR : 1); ++q)
-            if (q < units / C::NT) unit(threadIdx.x + q * C::NT);
+          for (int q = 0; q < (UNR > 0 ? UNR : 1); ++q) {
+            const int u = threadIdx.x + q * C::NT;
+            if (q < cdiv(units, C::NT) && (units % C::NT == 0 || u < units)) unit(u);
+          }
         } else {
 #pragma unroll 1
           for (int u = threadIdx.x; u < units; u += C::NT) unit(u);
