@@ -37,11 +37,6 @@ constexpr unsigned long long kDrainNs = 2000000000ull;
 #ifndef CSD_CHAIN_SKEW
 #define CSD_CHAIN_SKEW 1
 #endif
-// Strip loads as explicit 16-byte shared-memory loads on 32-bit shared
-// addresses (1) or as C++ loads through the ring pointer (0).
-#ifndef CSD_LDS_ASM
-#define CSD_LDS_ASM 0
-#endif
 // Unroll also unit counts that do not divide the block (last round predicated).
 #ifndef CSD_UNROLL_RAGGED
 #define CSD_UNROLL_RAGGED 1
@@ -175,18 +170,12 @@ __device__ __forceinline__ Strip<T, LO, HI, VEC> load_strip(const T* row, int x)
   constexpr int NV = (A1 - A0) / ALIGN;
   typedef typename VecOf<T>::type V;
   T buf[NV * ALIGN];
-#if CSD_LDS_ASM
-  const unsigned a = ptx::smem_addr(row + x + A0);
-#pragma unroll
-  for (int i = 0; i < NV; ++i) ptx::lds16(a + 16u * i, &buf[i * ALIGN]);
-#else
   const V* src = reinterpret_cast<const V*>(row + x + A0);
 #pragma unroll
   for (int i = 0; i < NV; ++i) {
     const V t = src[i];
     *reinterpret_cast<V*>(&buf[i * ALIGN]) = t;
   }
-#endif
   Strip<T, LO, HI, VEC> s;
 #pragma unroll
   for (int i = 0; i < VEC + HI - LO; ++i) s.v[i] = buf[i + (LO - A0)];

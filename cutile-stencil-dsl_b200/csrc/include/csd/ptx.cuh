@@ -75,16 +75,6 @@ __device__ __forceinline__ void tma_load_3d(unsigned dst, const void* tmap, int 
       : "memory");
 }
 
-// 16-byte load from shared memory at a 32-bit shared address (16-byte aligned).
-__device__ __forceinline__ void lds16(unsigned addr, double* v) {
-  asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v[0]), "=d"(v[1]) : "r"(addr));
-}
-__device__ __forceinline__ void lds16(unsigned addr, float* v) {
-  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
-               : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3])
-               : "r"(addr));
-}
-
 // 5-D TMA tile load into shared memory (bricked fields: x in brick, brick x,
 // y in brick, z in brick, brick y/z), completion counted on `bar`.
 __device__ __forceinline__ void tma_load_5d(unsigned dst, const void* tmap, int c0, int c1, int c2,
