@@ -223,23 +223,27 @@ def run_ours(args) -> dict:
 
     # end-to-end: pinned host field -> device, 50-sweep solve, result -> host
     # (bricked: the host holds the field in bricked form).  Solves run as a
-    # pipeline over two device buffer pairs on three streams, so one solve's
-    # copies overlap another's sweeps (two copy engines, one compute stream).
+    # pipeline over three device buffer pairs on three streams, so one solve's
+    # upload, another's sweeps and a third's download run at once (two copy
+    # engines, one compute stream); with two pairs an upload waited for the
+    # download of the solve before last and the copies could not both run
+    # all the time.
     if args.layout == "bricked":
         host_in = mod.to_bricks(torch.from_numpy(u0).cuda()).cpu().pin_memory()
     else:
         host_in = torch.from_numpy(u0).pin_memory()
-    host_outs = [torch.empty_like(host_in).pin_memory() for _ in range(2)]
-    pairs = [(a, b), (torch.empty_like(a), torch.empty_like(a))]
+    npairs = 3
+    host_outs = [torch.empty_like(host_in).pin_memory() for _ in range(npairs)]
+    pairs = [(a, b)] + [(torch.empty_like(a), torch.empty_like(a)) for _ in range(npairs - 1)]
     s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
-    ev = {k: [torch.cuda.Event(), torch.cuda.Event()] for k in ("h2d", "comp", "d2h")}
-    e2e_steps = 4
+    ev = {k: [torch.cuda.Event() for _ in range(npairs)] for k in ("h2d", "comp", "d2h")}
+    e2e_steps = 8
     sweeps = max(1, SOLVE_STEPS // T)
 
     def solve(k):
-        p = k % 2
+        p = k % npairs
         x, y = pairs[p]
-        if k >= 2:                      # the pair's previous solve is read out
+        if k >= npairs:                 # the pair's previous solve is read out
             s_in.wait_event(ev["d2h"][p])
         with torch.cuda.stream(s_in):
             x.copy_(host_in, non_blocking=True)
@@ -290,8 +294,9 @@ def run_ours(args) -> dict:
         "e2e": {"value": round(e2e_gpts, 3), "unit": "GPts/s",
                 "h2d_bytes_per_step": int(u0.nbytes), "d2h_bytes_per_step": int(u0.nbytes),
                 "step": f"H2D of the field, {sweeps} launches of launch_lap7 ({SOLVE_STEPS} steps),"
-                        f" D2H of the result; consecutive solves pipelined over two buffer pairs "
-                        f"(copies on two streams overlap the sweeps), wall time per solve"},
+                        f" D2H of the result; {e2e_steps} consecutive solves pipelined over "
+                        f"{npairs} buffer pairs (copies on two streams overlap the sweeps), wall "
+                        f"time per solve"},
         "gpu_launches": args.steps,
         "clocks": clocks,
         "cpu_baseline": cpu,
