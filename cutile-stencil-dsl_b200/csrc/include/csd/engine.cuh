@@ -37,6 +37,11 @@ constexpr unsigned long long kDrainNs = 2000000000ull;
 #ifndef CSD_CHAIN_SKEW
 #define CSD_CHAIN_SKEW 1
 #endif
+// A block barrier after every chunk wait (1), or only where a fused boundary
+// patch wrote into the chunk (0).
+#ifndef CSD_STEP_BARRIER
+#define CSD_STEP_BARRIER 1
+#endif
 // Unroll also unit counts that do not divide the block (last round predicated).
 #ifndef CSD_UNROLL_RAGGED
 #define CSD_UNROLL_RAGGED 1
@@ -747,8 +752,18 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
           patch_boundary<C>(g, ring, slot, cx, cy, cz + i * C::ROWS);
         }
       }
-      __syncthreads();
-      if (abort_flag) break;
+      // Each thread has waited for chunk i itself, so a barrier is needed
+      // here only when the boundary patch wrote into the chunk (other threads
+      // read those cells): refills are ordered by the barrier that ends every
+      // step, and chained stages read only what earlier steps (or, without
+      // the skewed schedule, the barrier between stages) completed.  Without
+      // it a failed wait is acted on at the end-of-step barrier (the step's
+      // results are discarded with the launch's).
+      constexpr bool kTopBarrier = C::BC != CSD_BC_NONE || CSD_STEP_BARRIER;
+      if constexpr (kTopBarrier) {
+        __syncthreads();
+        if (abort_flag) break;
+      }
 
       // stages 1..T: stage s computes chunk k_s = i - STAGE_OFF(s) of its
       // field; stage 1 reads input chunks up to i (landed above), stage
@@ -907,6 +922,9 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
       // every stage's reads of this step are done before the refill below
       // and before the next step overwrites a ring slot
       __syncthreads();
+      if constexpr (!kTopBarrier) {
+        if (abort_flag) break;
+      }
 
       // refill: input chunk i - 2*HC is dead, its slot takes chunk i - 2*HC + NSLOT
       {
