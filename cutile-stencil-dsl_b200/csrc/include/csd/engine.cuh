@@ -37,11 +37,6 @@ constexpr unsigned long long kDrainNs = 2000000000ull;
 #ifndef CSD_CHAIN_SKEW
 #define CSD_CHAIN_SKEW 1
 #endif
-// A block barrier after every chunk wait (1), or only where a fused boundary
-// patch wrote into the chunk (0).
-#ifndef CSD_STEP_BARRIER
-#define CSD_STEP_BARRIER 1
-#endif
 // Unroll also unit counts that do not divide the block (last round predicated).
 #ifndef CSD_UNROLL_RAGGED
 #define CSD_UNROLL_RAGGED 1
@@ -759,7 +754,10 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
       // the skewed schedule, the barrier between stages) completed.  Without
       // it a failed wait is acted on at the end-of-step barrier (the step's
       // results are discarded with the launch's).
-      constexpr bool kTopBarrier = C::BC != CSD_BC_NONE || CSD_STEP_BARRIER;
+      // Measured on 512^3: chains gain without it (FP64 T=2 351 -> 356, 8 x
+      // 128 tiles 359 -> 366 GPts/s); single-step kernels keep it (box27 266
+      // with it, 262 without; the 7-point sweeps equal).
+      constexpr bool kTopBarrier = C::BC != CSD_BC_NONE || T_ == 1;
       if constexpr (kTopBarrier) {
         __syncthreads();
         if (abort_flag) break;

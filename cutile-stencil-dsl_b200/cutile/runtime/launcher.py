@@ -575,11 +575,11 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
         # one row per thread over the wide tile instead
         plan = replace(plan, rpy=1, rows=1, tile_y=4, tile_x=64)
     if T > 1 and len(stencil_halo) == 3 and tile_sizes is None and not plan.rpy > 1:
-        # 3-D chains: 8 x 64 tiles, 128 threads (measured on 512^3 FP64, T=2:
-        # 307.6 GPts/s against 199.9 for the single-step default 4 x 128,
-        # whose larger rings leave 3 blocks per SM and 512 columns for 444
-        # resident slots)
-        plan = replace(plan, rows=1, tile_y=8, tile_x=64, threads=128)
+        # 3-D chains: 8 x 128 tiles, 256 threads (measured on 512^3 FP64, T=2,
+        # eight waves: 365.5 GPts/s; 8 x 64 / 128 threads 356.3; the
+        # single-step default 4 x 128 in one wave 199.9, its larger rings
+        # leaving 3 blocks per SM and 512 columns for 444 resident slots)
+        plan = replace(plan, rows=1, tile_y=8, tile_x=128, threads=256)
     elif T > 1 and len(stencil_halo) == 2 and tile_sizes is None:
         # 2-D chains (measured on heat 4096^2 FP64): T=2 over 8 x 64 chunks,
         # 128 threads, 346 GPts/s (8 x 128: 317); deeper chains over 4 x 128
