@@ -1385,9 +1385,9 @@ def run_sw_reference(args) -> dict | None:
 # as its own `bench.py` process (its own memory, its own clock samples) and
 # contributes a compact summary of its JSON line under "secondary".
 SECONDARY = (
-    ("lap7_fp32", ["--dtype", "float32", "--steps", "20"]),
-    ("lap7_fp64_T2", ["--temporal", "2", "--steps", "20"]),
-    ("lap7_fp64_bricked8", ["--layout", "bricked", "--steps", "20"]),
+    ("lap7_fp32", ["--dtype", "float32", "--steps", "100"]),
+    ("lap7_fp64_T2", ["--temporal", "2", "--steps", "50"]),
+    ("lap7_fp64_bricked8", ["--layout", "bricked", "--steps", "50"]),
     ("gray_scott_4096_kahan", ["--workload", "gray_scott", "--steps", "1000"]),
     ("heat_4096_small_step_kahan", ["--workload", "heat_kahan", "--steps", "2000"]),
     ("sw_batch_256", ["--workload", "sw_batch"]),
