@@ -37,11 +37,6 @@ constexpr unsigned long long kDrainNs = 2000000000ull;
 #ifndef CSD_CHAIN_SKEW
 #define CSD_CHAIN_SKEW 1
 #endif
-// Extra 16-byte columns of every staged row of single-step kernels (row pitch
-// experiments; 0 in the product).
-#ifndef CSD_BOXW_PAD
-#define CSD_BOXW_PAD 0
-#endif
 // Unroll also unit counts that do not divide the block (last round predicated).
 #ifndef CSD_UNROLL_RAGGED
 #define CSD_UNROLL_RAGGED 1
@@ -102,7 +97,7 @@ struct Cfg {
   static constexpr int PADL = BTMA ? align_up(RX, BRICK_B)
                             : TEMPORAL == 1 ? RXA : align_up(TEMPORAL * RX + 2 * ALIGN - 2, ALIGN);
   static constexpr int BOXW = BTMA ? align_up(PADL + TX + RX, BALIGN)
-                            : TEMPORAL == 1 ? align_up(PADL + TX + RX, ALIGN) + CSD_BOXW_PAD * ALIGN
+                            : TEMPORAL == 1 ? align_up(PADL + TX + RX, ALIGN)
                                             : align_up(PADL + TX + TEMPORAL * RX + 2 * ALIGN - 2, ALIGN);
   static_assert(BRICK_ == 0 || LOADER_ == CSD_LOADER_LDG ||
                     (BRICK_NDIM == 3 && ROWS_ == 1 && TEMPORAL_ == 1 && BC_ != CSD_BC_PERIODIC &&
