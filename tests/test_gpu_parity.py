@@ -311,3 +311,25 @@ def test_validate_and_benchmark_api():
     assert r.validate(atol=1e-12)
     b = r.benchmark(iters=3, warmup=1)
     assert b["time_ms"] > 0 and b["gpoints_per_s"] > 0
+
+
+@pytest.mark.parametrize("defines", [("-DCSD_CHAIN_SKEW=0",), ("-DCSD_UNROLL_RAGGED=0",),
+                                     ("-DCSD_UNROLL_UNITS=0",)])
+@pytest.mark.parametrize("name,ndim,T", [("lap7", 3, 2), ("heat2d", 2, 4)])
+def test_engine_schedule_switches_keep_chains_exact(monkeypatch, defines, name, ndim, T):
+    """The engine's alternative schedules (per-stage barriers instead of the
+    skewed chain, loop instead of unrolled units) compute the same bits."""
+    import cutile
+    from cutile.runtime import native
+
+    monkeypatch.setattr(native, "NVRTC_OPTIONS", native.NVRTC_OPTIONS + tuple(defines))
+    fn = D.CASES[name][0]
+    r = cutile.compile(_stencil(fn, ndim), temporal_steps=T, align_halo=False)
+    sizes = {2: (61, 90), 3: (21, 17, 46)}
+    shape = tuple(s + 2 * h for s, h in zip(sizes[ndim], r.halo_widths))
+    u = np.random.default_rng(7).standard_normal(shape)
+    (got,) = _run(r, [u])
+    want = O.temporal_launch(u, np.full(shape, np.nan), fn, ndim, r.halo_widths, T)
+    inner = _interior(shape, r.halo_widths)
+    assert np.array_equal(got[inner], want[inner])
+    _check_halo_untouched(got, r.halo_widths)
