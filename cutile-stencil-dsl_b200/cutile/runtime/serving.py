@@ -307,6 +307,10 @@ class StencilServer:
     def _wait(self, mark) -> None:
         mark.synchronize()
 
+    def _done(self, mark) -> bool:
+        """Whether the GPU has passed ``mark`` (no waiting)."""
+        return mark.query()
+
     def _mark_time(self, mark, start, t_start: float) -> float:
         """Seconds after the loop start at which the GPU passed ``mark``."""
         return t_start + start.elapsed_time(mark) / 1e3
@@ -337,31 +341,41 @@ class StencilServer:
         self._wait(start)           # the GPU clock's zero is the loop start
         t0 = time.perf_counter()
         st = self.stats
-        while queue or active or in_flight:
+        def admit_one() -> bool:
+            """Admit (or reject) the head of the queue if it has arrived and
+            fits; False when nothing could be done."""
+            nonlocal used
             now = time.perf_counter() - t0
+            if not queue or (realtime and queue[0].arrival > now):
+                return False
+            r = queue[0]
+            need = self.memory_of(r)
+            if need > self.budget:
+                queue.popleft()
+                results[r.rid].error = (f"needs {need} bytes, more than the "
+                                        f"{self.budget}-byte budget")
+                st.rejected += 1
+                return True
+            if used + need > self.budget:
+                return False                    # first come, first served
+            queue.popleft()
+            ta = time.perf_counter()
+            a = self._admit(r, results[r.rid], now)
+            st.admit_s += time.perf_counter() - ta
+            active.append(a)
+            used += a.nbytes
+            st.admitted += 1
+            return True
+
+        while queue or active or in_flight:
             # admit arrived requests in order while they fit (a bounded amount
             # of host time per pass while solves are running)
             admit_until = time.perf_counter() + self.admit_budget_s
-            while queue and (not realtime or queue[0].arrival <= now):
+            while queue:
                 if (active or in_flight) and time.perf_counter() > admit_until:
                     break
-                r = queue[0]
-                need = self.memory_of(r)
-                if need > self.budget:
-                    queue.popleft()
-                    results[r.rid].error = (f"needs {need} bytes, more than the "
-                                            f"{self.budget}-byte budget")
-                    st.rejected += 1
-                    continue
-                if used + need > self.budget:
-                    break                       # first come, first served
-                queue.popleft()
-                ta = time.perf_counter()
-                a = self._admit(r, results[r.rid], now)
-                st.admit_s += time.perf_counter() - ta
-                active.append(a)
-                used += a.nbytes
-                st.admitted += 1
+                if not admit_one():
+                    break
             st.peak_bytes = max(st.peak_bytes, used)
             st.max_active = max(st.max_active, len(active))
             if active:
@@ -390,9 +404,15 @@ class StencilServer:
                         keep.append(a)
                 active = keep
                 in_flight.append((mark, finished))
-            # keep one iteration in flight while the next is prepared
+            # keep one iteration in flight while the next is prepared; the
+            # host time until the oldest one finishes admits arrived requests
+            # (their set-up work queues behind the running iteration), so
+            # admission costs no GPU time unless the host is the slower side
             while in_flight and (len(in_flight) > 1 or not active):
                 mark, finished = in_flight.popleft()
+                while not self._done(mark):
+                    if not admit_one():
+                        break
                 tw = time.perf_counter()
                 self._wait(mark)
                 st.wait_s += time.perf_counter() - tw

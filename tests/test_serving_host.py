@@ -43,6 +43,9 @@ class FakeServer(StencilServer):
     def _mark_time(self, mark, start, t_start):
         return t_start + (mark - start)
 
+    def _done(self, mark):
+        return True
+
 
 KINDS = [SolveKind("heat2d", {}, 1), SolveKind("wave2d", {}, 2), SolveKind("lap7", {}, 1)]
 
@@ -129,3 +132,34 @@ def test_all_complete_for_any_budget_that_fits_the_largest(budget_mult):
     res = s.run(reqs, realtime=False)
     assert all(r.error is None and r.completed >= r.admitted for r in res)
     assert s.stats.admitted == len(reqs)
+
+
+class BusyGpuServer(FakeServer):
+    """A GPU that stays busy for a few polls per iteration: the loop admits
+    arrived requests while it waits."""
+
+    def __init__(self, kinds, budget, busy_polls=3):
+        super().__init__(kinds, budget)
+        self.busy_polls = busy_polls
+        self.polls = {}
+
+    def _done(self, mark):
+        n = self.polls.get(mark, 0)
+        self.polls[mark] = n + 1
+        return n >= self.busy_polls
+
+
+def test_admission_while_the_gpu_runs_keeps_fifo_and_budget():
+    reqs = [SolveRequest("heat2d", "float64", (66, 66), 3 + (i % 4), arrival=0.0) for i in range(20)]
+    per = FakeServer(KINDS, 1e12).memory_of(reqs[0])
+    s = BusyGpuServer(KINDS, 5 * per)
+    s.admit_budget_s = 0.0        # the pre-iteration pass admits at most one
+    res = s.run(reqs, realtime=False)
+    assert all(r.error is None for r in res)
+    assert s.stats.admitted == 20 and s.stats.peak_bytes <= 5 * per
+    admitted = sorted(range(20), key=lambda i: (res[i].admitted, i))
+    assert admitted == list(range(20))
+    # every iteration ran at most five solves and each solve ran its steps
+    assert max(len(it) for it in s.iterations) <= 5
+    for r, q in zip(res, reqs):
+        assert sum(r.rid in it for it in s.iterations) == q.steps
