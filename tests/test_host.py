@@ -515,3 +515,28 @@ def test_rows_per_thread_default_falls_back_when_it_would_spill():
     assert "rpy" not in r.kernel_hints
     r2 = cutile.compile(W.load_box("regular_box125", 2), temporal_blocking=False)
     assert r2.kernel_hints.get("rpy") == 2
+
+
+def test_body_unroll_choice():
+    """Small bodies let the engine unroll a stage's units; wide ones (many
+    strip groups, rows per thread, long bodies) keep the loop."""
+    import re
+    import tempfile
+
+    import cutile
+    import ref_corpus as RC
+    from cutile import stencil
+
+    def unroll(r):
+        return {int(m) for m in re.findall(r"static constexpr int UNROLL = (\d+);", r.cuda_source)}
+
+    assert unroll(cutile.compile(stencil(ndim=3, order=2)(D.lap7), temporal_blocking=False)) == {4}
+    assert unroll(cutile.compile(stencil(ndim=2)(D.heat2d), temporal_blocking=False)) == {4}
+    entries, _ = RC.load()
+    with tempfile.TemporaryDirectory() as tmp:
+        fn = RC.build(tmp, "wide_stencils/box125", entries["wide_stencils/box125"])
+        assert unroll(cutile.compile(fn, temporal_blocking=False)) == {0}
+    from cutile import RKIntegrator
+
+    rk = RKIntegrator(stencil(ndim=2, dtype="float32")(D.sw_rhs), "rk2").compile(boundary="reflecting")
+    assert unroll(rk) == {0}
