@@ -1387,6 +1387,11 @@ def run_sw_reference(args) -> dict | None:
 SECONDARY = (
     ("lap7_fp32", ["--dtype", "float32", "--steps", "100"]),
     ("lap7_fp64_T2", ["--temporal", "2", "--steps", "50"]),
+    ("lap7_fp64_T4", ["--temporal", "4", "--steps", "25"]),
+    ("lap7_fp64_T8", ["--temporal", "8", "--steps", "10"]),
+    ("lap7_fp32_T2", ["--dtype", "float32", "--temporal", "2", "--steps", "50"]),
+    ("lap7_fp32_T4", ["--dtype", "float32", "--temporal", "4", "--steps", "25"]),
+    ("lap7_fp32_T8", ["--dtype", "float32", "--temporal", "8", "--steps", "10"]),
     ("lap7_fp64_bricked8", ["--layout", "bricked", "--steps", "50"]),
     ("gray_scott_4096_kahan", ["--workload", "gray_scott", "--steps", "1000"]),
     ("heat_4096_small_step_kahan", ["--workload", "heat_kahan", "--steps", "2000"]),

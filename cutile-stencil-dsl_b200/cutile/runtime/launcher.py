@@ -445,6 +445,29 @@ def generate_module_code(name: str, cuda_source: str, spec: dict, *, fused_outpu
     return e.render()
 
 
+def chain_tile_3d(dtype_bytes: int, T: int) -> dict:
+    """Default column tile and block size of a 3-D chain of T steps.
+
+    Measured on B200, 7-point Laplacian 512^3, eight waves, GPts/s counting
+    every step (plan sweeps over 4..32 x 32..128 tiles and 64..512 threads):
+    FP64 T=2 8 x 128 / 256 threads 366 (16 x 64: 356; the single-step 4 x 128
+    default 200); FP64 T=4 16 x 64 / 512 threads 246 (8 x 64 / 256: 159);
+    FP32 T=2 8 x 128 / 128 threads 661 (/ 256: 622); FP32 T=4 32 x 64 / 512
+    threads 445 (8 x 128 / 256: 282); FP32 T=8 16 x 32 / 128 threads 137
+    (8 x 64: 122).  Past T=2 the rings leave one block per SM, and the
+    tallest tile that fits, with a thread per unit, beats smaller tiles at
+    higher occupancy: every stage recomputes 2(T - s) r halo rows per tile.
+    ``fit_plan`` shrinks the tile of wider footprints until it fits."""
+    if T == 2:
+        return (dict(tile_y=8, tile_x=128, threads=256) if dtype_bytes == 8 else
+                dict(tile_y=8, tile_x=128, threads=128))
+    if T <= 4:
+        return (dict(tile_y=16, tile_x=64, threads=512) if dtype_bytes == 8 else
+                dict(tile_y=32, tile_x=64, threads=512))
+    return (dict(tile_y=8, tile_x=32, threads=128) if dtype_bytes == 8 else
+            dict(tile_y=16, tile_x=32, threads=128))
+
+
 def _rpy_keeps_registers(stencil_fn, plan, stencil_halo, halo_widths, dtype, dtype_bytes,
                          num_inputs, T, body_ops, kahan) -> bool:
     """Whether the rows-per-thread default compiles without spills for this
@@ -575,11 +598,7 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
         # one row per thread over the wide tile instead
         plan = replace(plan, rpy=1, rows=1, tile_y=4, tile_x=64)
     if T > 1 and len(stencil_halo) == 3 and tile_sizes is None and not plan.rpy > 1:
-        # 3-D chains: 8 x 128 tiles, 256 threads (measured on 512^3 FP64, T=2,
-        # eight waves: 365.5 GPts/s; 8 x 64 / 128 threads 356.3; the
-        # single-step default 4 x 128 in one wave 199.9, its larger rings
-        # leaving 3 blocks per SM and 512 columns for 444 resident slots)
-        plan = replace(plan, rows=1, tile_y=8, tile_x=128, threads=256)
+        plan = replace(plan, rows=1, **chain_tile_3d(dtype_bytes, T))
     elif T > 1 and len(stencil_halo) == 2 and tile_sizes is None:
         # 2-D chains (measured on heat 4096^2 FP64): T=2 over 8 x 64 chunks,
         # 128 threads, 346 GPts/s (8 x 128: 317); deeper chains over 4 x 128

@@ -6,7 +6,8 @@ over 256 uneven grids), so each benchmarked configuration is also checked at
 its real size against the oracle:
 
 * 3-D 7-point Laplacian, 512^3 interior, N(0,1) seed 1, FP64 and FP32, two
-  sweeps through ping-pong buffers (compiled exactly as the benchmark does);
+  sweeps through ping-pong buffers (compiled exactly as the benchmark does),
+  and one four-step chained launch in each dtype;
 * 2-D Gray-Scott 4096^2 periodic, fused two-output step in FP64 and the
   FP32 Kahan-compensated step, from the seeded 20-square start;
 * 256 shallow-water grids, sizes log-uniform in 64..2048 (seed 3), FP32 with
@@ -61,6 +62,32 @@ def test_lap7_512_cubed_two_sweeps(dtype):
     from cutile.runtime import native
 
     assert native.error_word(reset=True) == 0
+
+
+@pytest.mark.parametrize("dtype,T", [("float64", 4), ("float32", 4)])
+def test_lap7_512_cubed_chain(dtype, T):
+    """One temporally blocked launch at 512^3 on the default chain plan (the
+    tallest tiles, one block per SM, eight waves of items)."""
+    import cutile
+    from cutile import stencil
+
+    torch = _torch()
+    r = cutile.compile(stencil(ndim=3, order=2, dtype=dtype)(D.lap7), temporal_steps=T)
+    assert r.temporal_steps == T
+    h = r.halo_widths
+    n = 512
+    shape = tuple(n + 2 * x for x in h)
+    u = np.zeros(shape, dtype=dtype)
+    inner = tuple(slice(x, s - x) for x, s in zip(h, shape))
+    u[inner] = np.random.default_rng(1).standard_normal((n, n, n)).astype(dtype)
+    a = torch.from_numpy(u).cuda()
+    b = torch.zeros_like(a)
+    getattr(r.load_module(), f"launch_{r.name}")(a, b)
+    torch.cuda.synchronize()
+    got = b.cpu().numpy()
+    del a, b
+    want = O.temporal_launch(u, np.zeros_like(u), D.lap7, 3, h, T)
+    assert np.array_equal(got[inner], want[inner])
 
 
 def _gs(precision):

@@ -313,6 +313,26 @@ def test_validate_and_benchmark_api():
     assert b["time_ms"] > 0 and b["gpoints_per_s"] > 0
 
 
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+@pytest.mark.parametrize("T", [2, 4, 8])
+def test_3d_chain_default_tiles_over_ragged_columns(dtype, T):
+    """The 3-D chain defaults (tiles up to 32 x 64, up to 512 threads) over a
+    grid of several ragged column tiles, both dtypes, bit-exact against T
+    oracle steps."""
+    import cutile
+
+    r = cutile.compile(_stencil(D.lap7, 3, dtype=dtype), temporal_steps=T, align_halo=False)
+    assert r.temporal_steps == T
+    shape = tuple(s + 2 * h for s, h in zip((11, 37, 141), r.halo_widths))
+    u = np.random.default_rng(13).standard_normal(shape).astype(dtype)
+    (got,) = _run(r, [u])
+    want = O.temporal_launch(u, np.full(shape, np.nan, dtype=dtype), D.lap7, 3, r.halo_widths, T)
+    assert want.dtype == np.dtype(dtype)
+    inner = _interior(shape, r.halo_widths)
+    assert np.array_equal(got[inner], want[inner])
+    _check_halo_untouched(got, r.halo_widths)
+
+
 @pytest.mark.parametrize("defines", [("-DCSD_CHAIN_SKEW=0",), ("-DCSD_UNROLL_RAGGED=0",),
                                      ("-DCSD_UNROLL_UNITS=0",)])
 @pytest.mark.parametrize("name,ndim,T", [("lap7", 3, 2), ("heat2d", 2, 4)])
