@@ -250,11 +250,13 @@ def default_engine_plan(ndim: int, num_loads: int, dtype_bytes: int, radius: tup
                 else:
                     plan = replace(plan, rows=2, tile_y=4, tile_x=128, threads=128, rpy=2)
     elif ndim == 2:
-        # short single-field bodies (5/9-point) run best with 128 threads per
-        # 8x128 tile (autotuned, heat 4096^2: FP32 27 vs 32 us per step);
-        # multi-field flux bodies keep 256
+        # short single-field bodies (5/9-point) over 8 x 128 tiles: FP32 runs
+        # best with 128 threads (heat 4096^2: 671 vs 574 GPts/s with 256),
+        # FP64 with 256 (351 vs 312: two 2-point units per thread instead
+        # of four); multi-field flux bodies keep 256
+        short = num_loads <= 8 and dtype_bytes == 4
         plan = EnginePlan(2, rows=4 if wide else 8, tile_y=1, tile_x=128, vec=vec,
-                          threads=128 if num_loads <= 8 else 256, stages=1, zchunk=0)
+                          threads=128 if short else 256, stages=1, zchunk=0)
         rz = radius[0]
         if rz > plan.rows:
             plan = replace(plan, rows=_align_up(rz, 4))

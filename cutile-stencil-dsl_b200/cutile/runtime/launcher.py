@@ -468,6 +468,27 @@ def chain_tile_3d(dtype_bytes: int, T: int) -> dict:
             dict(tile_y=16, tile_x=32, threads=128))
 
 
+def chain_tile_2d(dtype_bytes: int, T: int) -> dict:
+    """Default chunk (rows x columns) and block size of a 2-D chain of T steps.
+
+    Measured on B200, 5-point heat 4096^2, GPts/s counting every step (plan
+    sweeps over 4..32 rows, 64..256 columns, 128..512 threads; differences
+    under 5 % are kept at the simpler plan): FP64 T=2 8 x 64 / 128 threads
+    368, T=3 4 x 128 / 128 351 (/ 256: 328), T=4 4 x 128 / 256 302, T=5 259,
+    T=8 176; FP32 T=2 8 x 128 / 128 581 (8 x 64: 516), T=3 8 x 128 / 256
+    513 (4 x 128: 486), T=4 4 x 128 455, T=5 389, T=8 8 x 128 / 256 287
+    (4 x 128: 271)."""
+    if dtype_bytes == 8:
+        if T == 2:
+            return dict(rows=8, tile_x=64, threads=128)
+        return dict(rows=4, tile_x=128, threads=128 if T == 3 else 256)
+    if T == 2:
+        return dict(rows=8, tile_x=128, threads=128)
+    if T == 3 or T >= 8:
+        return dict(rows=8, tile_x=128, threads=256)
+    return dict(rows=4, tile_x=128, threads=256)
+
+
 def _rpy_keeps_registers(stencil_fn, plan, stencil_halo, halo_widths, dtype, dtype_bytes,
                          num_inputs, T, body_ops, kahan) -> bool:
     """Whether the rows-per-thread default compiles without spills for this
@@ -600,11 +621,7 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
     if T > 1 and len(stencil_halo) == 3 and tile_sizes is None and not plan.rpy > 1:
         plan = replace(plan, rows=1, **chain_tile_3d(dtype_bytes, T))
     elif T > 1 and len(stencil_halo) == 2 and tile_sizes is None:
-        # 2-D chains (measured on heat 4096^2 FP64): T=2 over 8 x 64 chunks,
-        # 128 threads, 346 GPts/s (8 x 128: 317); deeper chains over 4 x 128
-        # chunks, 256 threads, T=4 256 (8 x 128: 161, one block per SM)
-        plan = (replace(plan, rows=8, tile_x=64, threads=128) if T == 2 else
-                replace(plan, rows=4, tile_x=128, threads=256))
+        plan = replace(plan, **chain_tile_2d(dtype_bytes, T))
     if layout == "bricked" and len(stencil_halo) == 3 and tile_sizes is None:
         # one Z row per chunk, so that the bricked kernel can stage bricks
         # with tensor copies (target_to_cuda.brick_tma_eligible)

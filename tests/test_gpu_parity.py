@@ -333,6 +333,24 @@ def test_3d_chain_default_tiles_over_ragged_columns(dtype, T):
     _check_halo_untouched(got, r.halo_widths)
 
 
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+@pytest.mark.parametrize("T", [2, 3, 5, 8])
+def test_2d_chain_default_chunks_over_ragged_columns(dtype, T):
+    """The 2-D chain defaults per depth and dtype (4 or 8 rows by 64 or 128
+    columns, 128 or 256 threads) over several ragged column tiles."""
+    import cutile
+
+    r = cutile.compile(_stencil(D.heat2d, 2, dtype=dtype), temporal_steps=T, align_halo=False)
+    assert r.temporal_steps == T
+    shape = tuple(s + 2 * h for s, h in zip((75, 301), r.halo_widths))
+    u = np.random.default_rng(14).standard_normal(shape).astype(dtype)
+    (got,) = _run(r, [u])
+    want = O.temporal_launch(u, np.full(shape, np.nan, dtype=dtype), D.heat2d, 2, r.halo_widths, T)
+    inner = _interior(shape, r.halo_widths)
+    assert np.array_equal(got[inner], want[inner])
+    _check_halo_untouched(got, r.halo_widths)
+
+
 @pytest.mark.parametrize("defines", [("-DCSD_CHAIN_SKEW=0",), ("-DCSD_UNROLL_RAGGED=0",),
                                      ("-DCSD_UNROLL_UNITS=0",)])
 @pytest.mark.parametrize("name,ndim,T", [("lap7", 3, 2), ("heat2d", 2, 4)])

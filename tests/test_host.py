@@ -540,3 +540,31 @@ def test_body_unroll_choice():
 
     rk = RKIntegrator(stencil(ndim=2, dtype="float32")(D.sw_rhs), "rk2").compile(boundary="reflecting")
     assert unroll(rk) == {0}
+
+
+def test_measured_default_plans_per_dtype_and_depth():
+    """The plan tables: 2-D single steps (FP64 256 threads, FP32 128), 3-D
+    chains by depth (tallest tile that fits, a thread per unit past T=2), 2-D
+    chains by depth; what fit_plan returns for the 7-point and 5-point bodies."""
+    import cutile
+    from cutile import stencil
+
+    def plan(fn, ndim, dt, T):
+        kw = {"temporal_blocking": False} if T == 1 else {"temporal_steps": T}
+        r = cutile.compile(stencil(ndim=ndim, dtype=dt)(fn), **kw)
+        assert r.temporal_steps == T
+        return r.tile_sizes, r.kernel_hints["threads"]
+
+    assert plan(D.heat2d, 2, "float64", 1) == ((8, 128), 256)
+    assert plan(D.heat2d, 2, "float32", 1) == ((8, 128), 128)
+    assert plan(D.lap7, 3, "float64", 2) == ((1, 8, 128), 256)
+    assert plan(D.lap7, 3, "float64", 4) == ((1, 16, 64), 512)
+    assert plan(D.lap7, 3, "float64", 8) == ((1, 8, 32), 128)
+    assert plan(D.lap7, 3, "float32", 2) == ((1, 8, 128), 128)
+    assert plan(D.lap7, 3, "float32", 4) == ((1, 32, 64), 512)
+    assert plan(D.lap7, 3, "float32", 8) == ((1, 16, 32), 128)
+    assert plan(D.heat2d, 2, "float64", 2) == ((8, 64), 128)
+    assert plan(D.heat2d, 2, "float64", 3) == ((4, 128), 128)
+    assert plan(D.heat2d, 2, "float32", 2) == ((8, 128), 128)
+    assert plan(D.heat2d, 2, "float32", 3) == ((8, 128), 256)
+    assert plan(D.heat2d, 2, "float32", 8) == ((8, 128), 256)
