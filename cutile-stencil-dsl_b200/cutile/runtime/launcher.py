@@ -430,12 +430,13 @@ def generate_module_code(name: str, cuda_source: str, spec: dict, *, fused_outpu
                    f"brick_size, stream, scalars={sc})")
         e.blank()
         e.blank()
-        e.line(f"def launch_{name}_on_bricks({args}, shape, stream=None{kw}):")
+        e.line(f"def launch_{name}_on_bricks({args}, shape, stream=None{kw}, halo=None):")
         with e.indent():
             e.line('"""The bricked kernel on fields already stored as bricks of a ``shape`` '
-                   'array."""')
+                   'array')
+            e.line('(``halo``: the arrays\' halo widths, default ``halo_widths``)."""')
             e.line(f"_PROGRAM.launch_on_bricks(({', '.join(inputs)},), ({', '.join(outs)},), "
-                   f"shape, stream, scalars={sc})")
+                   f"shape, stream, scalars={sc}, halo=halo)")
     e.blank()
     e.blank()
     e.line("def program():")

@@ -190,11 +190,16 @@ class StencilProgram:
         return native.from_bricks(bricked, shape, int(brick_size), stream=stream)
 
     def launch_on_bricks(self, inputs, outputs, shape, stream=None, *,
-                         scalars: dict | None = None, loader: int = -1, zchunk: int = 0) -> None:
+                         scalars: dict | None = None, loader: int = -1, zchunk: int = 0,
+                         halo=None) -> None:
         """The bricked kernel on bricked fields of a ``shape`` array: writes
         the interior cells of the outputs' bricks (halo and padding cells
         untouched).  ``loader``: -1 picks TMA brick staging where the kernel
-        has it, else per-group cp.async copies."""
+        has it, else per-group cp.async copies.  ``halo``: the arrays' halo
+        widths when they differ from the compiled ``halo_widths`` (each at
+        least the stencil's reach); a halo of whole bricks starts the
+        interior on a brick, so that every column tile of the TMA staging
+        holds interior points."""
         bs = self._brick(self.spec["brick_size"])
         shape = tuple(int(n) for n in shape)
         if len(shape) != self.spec["ndim"]:
@@ -213,7 +218,11 @@ class StencilProgram:
                                 f"match the compiled dtype {want}")
         fin = [native.bricked_field(t, shape, bs) for t in inputs]
         fout = [native.bricked_field(t, shape, bs) for t in outputs]
-        native.launch_fields(self.kernel("bricked"), fin, fout, self.spec["halo"], stream,
+        halo = list(self.spec["halo"]) if halo is None else [int(h) for h in halo]
+        if len(halo) != len(shape):
+            raise ValueError(f"{self.spec['name']}: halo {halo} does not match the {len(shape)}-D "
+                             "shape")
+        native.launch_fields(self.kernel("bricked"), fin, fout, halo, stream,
                              loader=loader, zchunk=zchunk, scalars=self.scalar_values(scalars))
 
     def launch_bricked(self, inputs, outputs, brick_size, stream=None, *,

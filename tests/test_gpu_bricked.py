@@ -148,3 +148,36 @@ def test_bricked_box27_tma_staging():
     inner = tuple(slice(1, s - 1) for s in shape)
     assert np.array_equal(got[inner], want[inner])
     assert native.error_word(reset=True) == 0
+
+
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+@pytest.mark.parametrize("loader", [-1, 1])
+def test_brick_sized_halo_starts_the_interior_on_a_brick(dtype, loader):
+    """A field stored with a zero halo of one brick per side (the bench's
+    bricked layout), launched with ``halo=``: the interior, 13 x 37 x 150
+    cells from offset 8, equals the oracle's stencil on the same array;
+    nothing outside the interior is written."""
+    import torch
+
+    from cutile import compile as stencil_compile
+    from cutile import stencil
+
+    r = stencil_compile(stencil(ndim=3, dtype=dtype)(D.lap7), layout="bricked", brick_size=8,
+                        temporal_blocking=False)
+    assert r.halo_widths == (1, 1, 1)
+    halo = (8, 8, 8)
+    inner_n = (13, 37, 150)
+    shape = tuple(n + 2 * h for n, h in zip(inner_n, halo))
+    u = np.zeros(shape, dtype=dtype)
+    inner = tuple(slice(h, s - h) for h, s in zip(halo, shape))
+    u[inner] = np.random.default_rng(21).standard_normal(inner_n).astype(dtype)
+    mod = r.load_module()
+    ab = mod.to_bricks(torch.from_numpy(u).cuda())
+    ob = torch.full_like(ab, 7.0)
+    r.load_module().program().launch_on_bricks((ab,), (ob,), shape, loader=loader, halo=halo)
+    got = mod.from_bricks(ob, shape).cpu().numpy()
+    want = O.apply_stencil(u, D.lap7, 3, halo)
+    assert np.array_equal(got[inner], want[inner])
+    mask = np.ones(shape, bool)
+    mask[inner] = False
+    assert np.all(got[mask] == 7.0)
