@@ -568,3 +568,10 @@ def test_measured_default_plans_per_dtype_and_depth():
     assert plan(D.heat2d, 2, "float32", 2) == ((8, 128), 128)
     assert plan(D.heat2d, 2, "float32", 3) == ((8, 128), 256)
     assert plan(D.heat2d, 2, "float32", 8) == ((8, 128), 256)
+    from cutile import compile_fused
+
+    gs = [stencil(ndim=2)(D.gs_u), stencil(ndim=2)(D.gs_v)]
+    r = compile_fused(gs, precision="fp64", boundary="periodic")
+    assert (r.tile_sizes, r.kernel_hints["threads"]) == ((8, 64), 256)
+    r = compile_fused(gs, precision="fp32", boundary="periodic")
+    assert (r.tile_sizes, r.kernel_hints["threads"]) == ((8, 128), 256)
