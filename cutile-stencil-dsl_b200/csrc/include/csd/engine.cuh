@@ -66,7 +66,7 @@ __host__ __device__ constexpr int imax(int a, int b) { return a > b ? a : b; }
 // ---------------------------------------------------------------------------
 template <typename T_, int NIN_, int NOUT_, int RZ_, int RY_, int RX_, int ROWS_, int TY_, int TX_,
           int NT_, int STAGES_, int TEMPORAL_, int LOADER_, int BC_, int REDUCE_ = 0,
-          int BRICK_ = 0, int RPY_ = 1>
+          int BRICK_ = 0, int RPY_ = 1, int VEC_ = 0>
 struct Cfg {
   typedef T_ T;
   // Bricked layout: BRICK_ = (ndim << 4) | log2(brick size), 0 = flat.
@@ -88,14 +88,20 @@ struct Cfg {
   // the strip of row y + 1 at offset dy once for both rows that need it
   static constexpr int RPY = RPY_;
   static constexpr int ALIGN = 16 / (int)sizeof(T);
-  static constexpr int VEC = ALIGN;
+  // points per unit along X: one 16-byte vector by default; a wider unit
+  // (several vectors) reads each staged row group with fewer strips per
+  // point, for single-step flat kernels with one row per thread
+  static constexpr int VEC = VEC_ > 0 ? VEC_ : ALIGN;
+  static_assert(VEC % ALIGN == 0 &&
+                    (VEC == ALIGN || (TEMPORAL_ == 1 && BRICK_ == 0 && RPY_ == 1)),
+                "units wider than one vector: single-step flat kernels, one row per thread");
   static constexpr int HC = RZ > 0 ? cdiv(RZ, ROWS) : 0;  // halo chunks per side, per step
   // Column layout shared by every buffer: smem column c <-> x = X0 - PADL + c.
-  static constexpr int RXA = align_up(RX, ALIGN);
   // bricked TMA rows: whole bricks, each row 128-byte aligned (TMA destination)
   static constexpr int BALIGN = imax(BRICK_B, 128 / (int)sizeof(T));
   static constexpr int PADL = BTMA ? align_up(RX, BRICK_B)
-                            : TEMPORAL == 1 ? RXA : align_up(TEMPORAL * RX + 2 * ALIGN - 2, ALIGN);
+                            : TEMPORAL == 1 ? align_up(RX, VEC)
+                                            : align_up(TEMPORAL * RX + 2 * ALIGN - 2, ALIGN);
   static constexpr int BOXW = BTMA ? align_up(PADL + TX + RX, BALIGN)
                             : TEMPORAL == 1 ? align_up(PADL + TX + RX, ALIGN)
                                             : align_up(PADL + TX + TEMPORAL * RX + 2 * ALIGN - 2, ALIGN);
@@ -222,6 +228,13 @@ __device__ __forceinline__ void store_vec(double* p, const double* v) {
 }
 __device__ __forceinline__ void store_vec(float* p, const float* v) {
   *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+// One unit's VEC points as 16-byte vector stores.
+template <int VEC, typename T>
+__device__ __forceinline__ void store_unit(T* p, const T* v) {
+  constexpr int A = 16 / (int)sizeof(T);
+#pragma unroll
+  for (int i = 0; i < VEC; i += A) store_vec(p + i, v + i);
 }
 
 // Fused boundary fill: map an out-of-interior index of one dim to the
@@ -851,7 +864,7 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
                 for (int f = 0; f < C::NOUT; ++f) {
                   T* out = outp[f] + rowoff;
                   if (full && vec_store) {
-                    store_vec(out + gx0, ov[f]);
+                    store_unit<C::VEC>(out + gx0, ov[f]);
                   } else {
 #pragma unroll
                     for (int e = 0; e < C::VEC; ++e) {
@@ -866,7 +879,7 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
 #pragma unroll
                 for (int f = 0; f < C::NOUT; ++f) {
                   if (full && vec_store) {
-                    store_vec(outp[f] + off0, ov[f]);
+                    store_unit<C::VEC>(outp[f] + off0, ov[f]);
                   } else {
 #pragma unroll
                     for (int e = 0; e < C::VEC; ++e) {
@@ -886,7 +899,7 @@ __device__ __forceinline__ void engine_items(const csd_params& p, typename C::T*
                 T* d = dst + f * C::NSLOT_I * C::ISLOT_ELEMS(s) + (r * hs + y + j) * C::BOXW +
                        xv * C::VEC;
                 if (whole) {
-                  store_vec(d, ov[f]);
+                  store_unit<C::VEC>(d, ov[f]);
                 } else {
 #pragma unroll
                   for (int e = 0; e < C::VEC; ++e) {

@@ -198,8 +198,9 @@ def emit_body(kernel: KernelOp) -> str:
     dtype = kernel.dtype.data
     field_t = "f32" if dtype in ("float32", "fp32") else "f64"
     store_t = "float" if field_t == "f32" else "double"
-    vec = 4 if field_t == "f32" else 2   # 16 bytes of points per thread (engine Cfg::VEC)
-    rpy = engine_params(kernel)["RPY"]   # Y rows per thread (engine Cfg::RPY)
+    params = engine_params(kernel)
+    vec = params["VEC"]   # X points per unit (engine Cfg::VEC; 16 bytes unless widened)
+    rpy = params["RPY"]   # Y rows per thread (engine Cfg::RPY)
     accesses = [tuple(a.data for a in acc) for acc in kernel.accesses.data]
     acc_info = [_internal_offsets(ndim, offs) + (f,) for f, *offs in accesses]  # (dz, dy, dx, f)
     # strip groups: (field, dz, dy of the unit's row 0) -> X range, over all rows
@@ -360,6 +361,7 @@ def engine_params(kernel: KernelOp) -> dict:
         "REDUCE": kernel.reduce_max.data if kernel.reduce_max is not None else 0,
         "BRICK": _brick_code(kernel, ndim),
         "RPY": int(hints.get("rpy", 1)),
+        "VEC": int(hints.get("vec", 4 if dtype in ("float32", "fp32") else 2)),
     }
 
 
@@ -422,7 +424,7 @@ def emit_cuda(module: ModuleOp, preamble: bool = True) -> str:
                 loader = "CSD_LOADER_LDG"   # bricked fields the TMA boxes cannot stage
             cfg = (f"csd::Cfg<{p['T']}, {p['NIN']}, {p['NOUT']}, {p['RZ']}, {p['RY']}, {p['RX']}, "
                    f"{p['ROWS']}, {p['TY']}, {p['TX']}, {p['NT']}, {p['STAGES']}, {p['TEMPORAL']}, "
-                   f"{loader}, {p['BC']}, {p['REDUCE']}, {p['BRICK']}, {p['RPY']}>")
+                   f"{loader}, {p['BC']}, {p['REDUCE']}, {p['BRICK']}, {p['RPY']}, {p['VEC']}>")
             parts.append(f"typedef {cfg} Cfg_{name}_{suffix};")
             parts.append(f'extern "C" __global__ void __launch_bounds__({p["NT"]}, {p["MINB"]})')
             parts.append(f"{name}_{suffix}(const __grid_constant__ csd_params p) {{")

@@ -193,9 +193,8 @@ def engine_geometry(plan: EnginePlan, radius3: tuple[int, int, int], dtype_bytes
     T = plan.temporal
     align = 16 // dtype_bytes
     hc = -(-rz // plan.rows) if rz > 0 else 0
-    rxa = _align_up(rx, align)
     if T == 1:
-        pad_left = rxa
+        pad_left = _align_up(rx, max(align, plan.vec))   # Cfg::PADL: a unit starts on a vector
         box_w = _align_up(pad_left + plan.tile_x + rx, align)
     else:
         pad_left = _align_up(T * rx + 2 * align - 2, align)
@@ -287,6 +286,10 @@ def fit_plan(plan: EnginePlan, radius: tuple[int, ...], dtype_bytes: int,
     r3 = radius3(plan.ndim, radius)
     if plan.rpy != 1 and (plan.ndim != 3 or plan.temporal != 1 or plan.rpy < 1):
         raise ValueError("rows per thread > 1 needs a 3-D single-step stencil")
+    if plan.vec != 16 // dtype_bytes and (plan.vec % (16 // dtype_bytes) or plan.vec <= 0
+                                          or plan.temporal != 1 or plan.rpy != 1):
+        raise ValueError(f"a {plan.vec}-point unit needs a multiple of {16 // dtype_bytes} points, "
+                         "one step and one row per thread")
     for _ in range(64):
         g = engine_geometry(plan, r3, dtype_bytes, num_inputs, periodic)
         ok_box = g["box_w"] <= TMA_BOX_MAX and g["box_h"] <= TMA_BOX_MAX

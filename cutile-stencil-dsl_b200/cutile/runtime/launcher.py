@@ -335,7 +335,7 @@ def _plan_from(tile_sizes, kernel_hints, ndim, base_plan):
             p = replace(p, tile_x=t[0])
     if kernel_hints:
         kw = {}
-        for k in ("threads", "stages", "zchunk", "waves"):
+        for k in ("threads", "stages", "zchunk", "waves", "vec"):
             if k in kernel_hints:
                 kw[k] = int(kernel_hints[k])
         # "rows_per_thread" is the documented hint; "rpy" is the key
@@ -631,6 +631,8 @@ def compile(stencil_fn, domain: tuple[int, ...] | None = None, hw=None,
     if occupancy is not None:
         plan = replace(plan, occupancy=int(occupancy))
     plan = fit_plan(plan, stencil_halo, dtype_bytes, num_inputs, analysis.get("body_ops", 0))
+    if layout == "bricked" and plan.vec != 16 // dtype_bytes:
+        raise ValueError("bricked kernels keep one 16-byte vector per unit")
     verify_engine_plan(clone, plan, stencil_halo, dtype_bytes, num_inputs)
     hints = plan.hints()
     if occupancy is not None:

@@ -351,6 +351,28 @@ def test_2d_chain_default_chunks_over_ragged_columns(dtype, T):
     _check_halo_untouched(got, r.halo_widths)
 
 
+@pytest.mark.parametrize("name,ndim,dtype,tile,vec,threads", [
+    ("lap7", 3, "float32", (2, 8, 128), 8, 128), ("lap7", 3, "float64", (1, 4, 128), 4, 64),
+    ("heat2d", 2, "float64", (8, 128), 4, 128), ("heat2d", 2, "float32", (16, 128), 8, 128)])
+def test_wider_units_are_bit_exact(name, ndim, dtype, tile, vec, threads):
+    """Units of two 16-byte vectors (``kernel_hints={"vec": ...}``) over
+    ragged column tiles: same bits as the oracle, halo untouched."""
+    import cutile
+
+    fn = D.CASES[name][0]
+    r = cutile.compile(_stencil(fn, ndim, dtype=dtype), temporal_blocking=False,
+                       tile_sizes=tile, kernel_hints={"vec": vec, "threads": threads})
+    assert r.kernel_hints["vec"] == vec
+    size = {3: (13, 37, 150), 2: (75, 301)}[ndim]
+    shape = tuple(s + 2 * h for s, h in zip(size, r.halo_widths))
+    u = np.random.default_rng(5).standard_normal(shape).astype(dtype)
+    (got,) = _run(r, [u])
+    want = O.apply_stencil(u, fn, ndim, r.halo_widths)
+    inner = _interior(shape, r.halo_widths)
+    assert np.array_equal(got[inner], want[inner])
+    _check_halo_untouched(got, r.halo_widths)
+
+
 @pytest.mark.parametrize("defines", [("-DCSD_CHAIN_SKEW=0",), ("-DCSD_UNROLL_RAGGED=0",),
                                      ("-DCSD_UNROLL_UNITS=0",)])
 @pytest.mark.parametrize("name,ndim,T", [("lap7", 3, 2), ("heat2d", 2, 4)])

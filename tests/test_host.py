@@ -396,7 +396,7 @@ def test_rows_per_thread_plans():
 
     r27 = stencil_compile(W.load_box("box27_plan", 1), temporal_blocking=False)
     assert r27.tile_sizes == (1, 16, 64) and r27.kernel_hints["rpy"] == 4
-    assert ", 4> Cfg_box27_plan_tma;" in r27.cuda_source
+    assert ", 4, 2> Cfg_box27_plan_tma;" in r27.cuda_source   # RPY 4, VEC 2
     r125 = stencil_compile(W.load_box("box125_plan", 2), temporal_blocking=False)
     assert r125.tile_sizes == (2, 4, 128) and r125.kernel_hints["rpy"] == 2
     assert "rpy" not in stencil_compile(W.load_box("box27_plan", 1)).kernel_hints  # T = 2
@@ -575,3 +575,23 @@ def test_measured_default_plans_per_dtype_and_depth():
     assert (r.tile_sizes, r.kernel_hints["threads"]) == ((8, 64), 256)
     r = compile_fused(gs, precision="fp32", boundary="periodic")
     assert (r.tile_sizes, r.kernel_hints["threads"]) == ((8, 128), 256)
+
+
+def test_wider_units_only_for_single_step_flat_one_row_kernels():
+    import pytest as _pytest
+
+    import cutile
+    from cutile import stencil
+
+    lap = stencil(ndim=3, order=2)(D.lap7)
+    r = cutile.compile(lap, temporal_blocking=False, tile_sizes=(1, 4, 128),
+                       kernel_hints={"vec": 4, "threads": 64})
+    assert r.kernel_hints["vec"] == 4 and ", 1, 4> Cfg_lap7_tma;" in r.cuda_source
+    with _pytest.raises(ValueError):
+        cutile.compile(lap, temporal_steps=2, tile_sizes=(1, 8, 128), kernel_hints={"vec": 4})
+    with _pytest.raises(ValueError):
+        cutile.compile(lap, temporal_blocking=False, tile_sizes=(1, 4, 128),
+                       kernel_hints={"vec": 3})
+    with _pytest.raises(ValueError):
+        cutile.compile(lap, temporal_blocking=False, layout="bricked", brick_size=8,
+                       tile_sizes=(1, 4, 128), kernel_hints={"vec": 4})
