@@ -242,7 +242,7 @@ def run_ours(args) -> dict:
     pairs = [(a, b)] + [(torch.empty_like(a), torch.empty_like(a)) for _ in range(npairs - 1)]
     s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
     ev = {k: [torch.cuda.Event() for _ in range(npairs)] for k in ("h2d", "comp", "d2h")}
-    e2e_steps = 16
+    e2e_steps = 32
     sweeps = max(1, SOLVE_STEPS // T)
 
     def solve(k):
