@@ -40,7 +40,8 @@ def test_lap7_rows_per_thread(rpy, tile, dtype, size):
 
     r = cutile.compile(stencil(ndim=3, dtype=dtype)(D.lap7), temporal_blocking=False,
                        tile_sizes=tile, kernel_hints={"rows_per_thread": rpy, "threads": 128})
-    assert f", {rpy}> Cfg_lap7_tma" in r.cuda_source
+    vec = 4 if dtype == "float32" else 2
+    assert f", {rpy}, {vec}> Cfg_lap7_tma" in r.cuda_source   # RPY, VEC
     shape = tuple(s + 2 * h for s, h in zip(size, r.halo_widths))
     u = np.random.default_rng(sum(size) + rpy).standard_normal(shape).astype(dtype)
     got = _launch(r, [u])
