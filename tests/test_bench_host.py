@@ -47,3 +47,35 @@ def test_secondary_reports_a_failing_child(monkeypatch):
     monkeypatch.setattr(subprocess, "run", lambda *a, **k: Done())
     res = bench.run_secondary(budget_s=100)
     assert res["broken"]["error"].startswith("rc=1") and "no device" in res["broken"]["error"]
+
+
+def test_traffic_records_match_the_algorithmic_bytes():
+    """Each committed DRAM-traffic record (ncu at 320^3, scaled to 512^3) is
+    within 10 % of one read and one write of the field per launch: the
+    kernels re-read nothing, and a stale record would show here."""
+    import bench
+
+    for dtype, size in (("float64", 8), ("float32", 4)):
+        for T in (1, 2, 4):
+            for layout in ("flat", "bricked"):
+                t = bench._profiled_traffic(dtype, T, layout)
+                if t is None:
+                    continue
+                alg = 2 * size * 512 ** 3
+                assert 0.9 * alg <= t <= 1.1 * alg, (dtype, T, layout, t / alg)
+    assert bench._profiled_traffic("float64", 1) is not None
+    assert bench._profiled_traffic("float64", 1, "bricked") is not None
+
+
+def test_secondary_lines_cover_the_sweep_variants():
+    """The 7-point configuration's variants: FP32, chains of 2, 4 and 8 steps
+    in both dtypes, resident 8^3 bricks."""
+    import bench
+
+    args = {name: " ".join(extra) for name, extra in bench.SECONDARY}
+    for dt in ("", "--dtype float32 "):
+        for T in (2, 4, 8):
+            assert any(a.startswith(f"{dt}--temporal {T} ") or a == f"{dt}--temporal {T}"
+                       for a in args.values()), (dt, T)
+    assert any("--layout bricked" in a for a in args.values())
+    assert any(a.startswith("--dtype float32 --steps") for a in args.values())
