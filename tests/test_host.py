@@ -595,3 +595,20 @@ def test_wider_units_only_for_single_step_flat_one_row_kernels():
     with _pytest.raises(ValueError):
         cutile.compile(lap, temporal_blocking=False, layout="bricked", brick_size=8,
                        tile_sizes=(1, 4, 128), kernel_hints={"vec": 4})
+
+
+def test_bricked_wrapper_takes_the_arrays_halo():
+    """``launch_<name>_on_bricks`` passes a ``halo=`` override to the
+    program (a halo of whole bricks starts the interior on a brick)."""
+    import inspect
+
+    import cutile
+    from cutile import stencil
+
+    r = cutile.compile(stencil(ndim=3)(D.lap7), layout="bricked", brick_size=8,
+                       temporal_blocking=False)
+    assert "def launch_lap7_on_bricks(u_in, u_out, shape, stream=None, halo=None):" in r.code
+    assert "shape, stream, scalars=None, halo=halo)" in r.code
+    from cutile.runtime.module import StencilProgram
+
+    assert "halo" in inspect.signature(StencilProgram.launch_on_bricks).parameters
